@@ -1,0 +1,157 @@
+/*
+ * quick_b200.h -- C ABI of the B200-native two-electron Fock build ("get2e").
+ *
+ * Two layers share one implementation:
+ *
+ * 1. Drop-in entry points with the names, argument order and by-reference
+ *    calling convention of QUICK's own GPU shim (gfortran-style trailing
+ *    underscore), so QUICK's unchanged Fortran SCF driver links against this
+ *    library instead of the reference's get2e.  They act on one process-wide
+ *    default context, exactly like the reference's global `gpu` object
+ *    (src/gpu/cuda/gpu_type.h:512).  Like the reference they return no status
+ *    (except where the reference has an `ierr`); `qk_last_status()` reports
+ *    the most recent failure.
+ *
+ * 2. A context API (`qk_*`) with explicit handles, status returns, device
+ *    pointers and CUDA streams, for callers that batch several molecules or
+ *    keep data resident on the GPU.
+ *
+ * Array conventions on the drop-in layer are QUICK's: Fortran column-major,
+ * 1-based index values, MAXPRIM rows in gccoeff/gcexpo (20, the f-enabled
+ * build; see qk_set_maxprim).  No torch types appear anywhere in this ABI.
+ */
+#ifndef QUICK_B200_H
+#define QUICK_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- statuses */
+enum {
+    QK_OK = 0,
+    QK_ERR_NO_DEVICE = 24,        /* same code as gpu_init_device_ (src/gpu/cuda/gpu.cu:291-330) */
+    QK_ERR_INVALID_ARG = 101,
+    QK_ERR_NOT_READY = 102,       /* a required upload has not happened yet */
+    QK_ERR_CUDA = 103,
+    QK_ERR_OUT_OF_MEMORY = 104,
+    QK_ERR_UNSUPPORTED = 105,     /* e.g. angular momentum above the compiled maximum */
+    QK_ERR_BASIS_LAYOUT = 106     /* KLMN / cons do not follow QUICK's convention */
+};
+
+/* ======================================================= drop-in entry points */
+
+/* replaces gpu_new_ (src/gpu/cuda/gpu.cu:197) */
+void gpu_new_(int *ierr);
+/* replaces gpu_set_device_ (src/gpu/cuda/gpu.h:14) */
+void gpu_set_device_(int *gpuid, int *ierr);
+/* replaces gpu_init_device_ (src/gpu/cuda/gpu.cu:281) */
+void gpu_init_device_(int *ierr);
+/* replaces gpu_allocate_scratch_ (src/gpu/cuda/gpu.cu:437); nothing to allocate here */
+void gpu_allocate_scratch_(bool *allocate_gradient_scratch);
+/* replaces gpu_deallocate_scratch_ (src/gpu/cuda/gpu.cu:496) */
+void gpu_deallocate_scratch_(bool *deallocate_gradient_scratch);
+/* replaces gpu_setup_ (src/gpu/cuda/gpu.cu:539) */
+void gpu_setup_(int *natom, int *nbasis, int *nElec, int *imult, int *molchg, int *iAtomType);
+/* replaces gpu_upload_method_ (src/gpu/cuda/gpu.cu:722); only HF (method 0) has exchange 1.0 */
+void gpu_upload_method_(int *quick_method, bool *is_oshell, double *hyb_coeff);
+/* replaces gpu_upload_xyz_ (src/gpu/cuda/gpu.cu:776); xyz(3,natom) in Bohr */
+void gpu_upload_xyz_(double *atom_xyz);
+/* replaces gpu_upload_atom_and_chg_ (src/gpu/cuda/gpu.cu:820) */
+void gpu_upload_atom_and_chg_(int *atom, double *atom_chg);
+/* replaces gpu_upload_basis_ (src/gpu/cuda/gpu.cu:1782), same 29 arguments */
+void gpu_upload_basis_(int *nshell, int *nprim, int *jshell, int *jbasis, int *maxcontract,
+                       int *ncontract, int *itype, double *aexp, double *dcoeff,
+                       int *first_basis_function, int *last_basis_function,
+                       int *first_shell_basis_function, int *last_shell_basis_function,
+                       int *ncenter, int *kstart, int *katom, int *ktype, int *kprim, int *kshell,
+                       int *Ksumtype, int *Qnumber, int *Qstart, int *Qfinal, int *Qsbasis,
+                       int *Qfbasis, double *gccoeff, double *cons, double *gcexpo, int *KLMN);
+/* replaces gpu_upload_cutoff_matrix_ (src/gpu/cuda/gpu.cu:879): YCutoff(nshell,nshell),
+ * cutPrim(jbasis,jbasis) as computed by schwarzoff */
+void gpu_upload_cutoff_matrix_(double *YCutoff, double *cutPrim);
+/* replaces gpu_upload_calculated_ (src/gpu/cuda/gpu.cu:1690): density `dense` (nbasis^2) */
+void gpu_upload_calculated_(double *o, double *co, double *vec, double *dense);
+/* replaces gpu_upload_cutoff_ (src/gpu/cuda/gpu.cu:840): cutMatrix(nshell,nshell) and cutoffs */
+void gpu_upload_cutoff_(double *cutMatrix, double *integralCutoff, double *primLimit,
+                        double *DMCutoff, double *coreIntegralCutoff);
+/* replaces gpu_get_cshell_eri_ (src/gpu/gpu_get2e_getxc_drivers.h:27, declared at
+ * src/gpu/cuda/gpu.h:65): o(nbasis,nbasis) += G(dense), G = J - K/2 */
+void gpu_get_cshell_eri_(bool *deltaO, double *o);
+/* replaces gpu_delete_ (src/gpu/cuda/gpu.cu:514) */
+void gpu_delete_(int *ierr);
+
+/* ======================================================= context API */
+typedef struct qk_ctx qk_ctx;
+
+/* Status of the most recent failing call on the default (drop-in) context. */
+int qk_last_status(void);
+const char *qk_status_string(int status);
+/* Rows of gccoeff/gcexpo expected by gpu_upload_basis_ (reference MAXPRIM; default 20). */
+int qk_set_maxprim(int maxprim);
+/* Largest angular momentum per shell compiled into the kernels (2 = d). */
+int qk_max_l(void);
+
+/* Create / destroy a context on CUDA device `device`. */
+qk_ctx *qk_create(int device, int *status);
+int qk_destroy(qk_ctx *ctx);
+/* The process-wide context the drop-in entry points use (created on first use). */
+qk_ctx *qk_default_ctx(void);
+
+/* Molecule + basis in QUICK layout (arguments as in gpu_upload_basis_, restricted to
+ * what get2e needs).  xyz(3,natom) Bohr; kstart/katom/kprim/Ksumtype 1-based. */
+int qk_set_basis(qk_ctx *ctx, int natom, const double *xyz, int nshell, int nbasis, int jbasis,
+                 const int *kstart, const int *katom, const int *kprim, const int *Ksumtype,
+                 const int *Qstart, const int *Qfinal, const int *Qsbasis, const int *Qfbasis,
+                 const double *gccoeff, const double *cons, const double *gcexpo,
+                 const int *KLMN, int maxprim);
+
+/* Schwarz bounds on the GPU (replaces schwarzoff, src/modules/quick_cutoff_module.f90:54-89):
+ * YCutoff(nshell,nshell) and cutPrim(jbasis,jbasis) written to host arrays (may be NULL)
+ * and installed in the context. */
+int qk_schwarz(qk_ctx *ctx, double *YCutoff, double *cutPrim);
+/* Install caller-provided Schwarz bounds (same layout as gpu_upload_cutoff_matrix_). */
+int qk_set_schwarz(qk_ctx *ctx, const double *YCutoff, const double *cutPrim);
+/* integralCutoff and primLimit (src/modules/quick_method_module.f90:772-775). */
+int qk_set_cutoffs(qk_ctx *ctx, double integralCutoff, double primLimit);
+
+/* o_dev += G(D_dev).  D_dev, o_dev: nbasis^2 FP64 on the device.  cutmat_dev: nshell^2
+ * density screen (max |D| per shell pair) or NULL to derive it from D_dev on the device
+ * (cshell_density_cutoff, src/modules/include/cutoff.fh:62-92).  Enqueued on `stream`
+ * (a cudaStream_t; NULL = the CUDA default stream); returns without synchronising.
+ * The first call after a basis, Schwarz or cutoff change also builds the pair tables
+ * and work lists on the host and waits for their upload. */
+int qk_fock2e_device(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
+                     double *o_dev, void *stream);
+/* Same with host buffers (copies D in, adds G into o, synchronises). */
+int qk_fock2e_host(qk_ctx *ctx, const double *D, const double *cutmat, double *o);
+/* Density screen on the device: cutmat_dev(nshell,nshell) = max |D| per shell pair
+ * (stream: a cudaStream_t, NULL = the CUDA default stream). */
+int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_dev, void *stream);
+
+/* Work statistics of the last build: shell quartets listed and primitive quartets
+ * listed after Schwarz screening (before density screening). */
+int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int *launches);
+/* Kernel launches of one build (for launch accounting). */
+int qk_launches_per_build(qk_ctx *ctx);
+
+/* One-electron integrals on device `device` (replaces the get1e path and the
+ * reference's gpu_get_oei_, src/gpu/gpu_oei.cu:194; CPU twin
+ * src/modules/quick_oei_module.f90:69-257).  Basis in QUICK's normalize_basis
+ * layout: ncontract(nbasis), itype(3,nbasis), aexp/dcoeff(maxcontract,nbasis),
+ * ncenter(nbasis) 1-based.  Charges: nuclei Z(natom) at xyz(3,natom) plus `next`
+ * external point charges ext_q at ext_xyz(3,next) (QM/MM).  Writes S, T, V
+ * (nbasis^2, symmetric) to host arrays; functions up to d. */
+int qk_oei_host(int device, int natom, const double *xyz, const double *Z, int nbasis,
+                int maxcontract, const int *ncontract, const int *itype, const double *aexp,
+                const double *dcoeff, const int *ncenter, int next, const double *ext_xyz,
+                const double *ext_q, double *S, double *T, double *V);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QUICK_B200_H */

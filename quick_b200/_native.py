@@ -1,0 +1,82 @@
+"""ctypes binding of libquick_b200.so (the C ABI declared in include/quick_b200.h).
+
+The library is the product's only compute path: if it is missing the import of
+this module fails with an error naming the build step; there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libquick_b200.so")
+
+# every symbol include/quick_b200.h declares
+EXPORTED = [
+    "gpu_new_", "gpu_set_device_", "gpu_init_device_", "gpu_allocate_scratch_",
+    "gpu_deallocate_scratch_", "gpu_setup_", "gpu_upload_method_", "gpu_upload_xyz_",
+    "gpu_upload_atom_and_chg_", "gpu_upload_basis_", "gpu_upload_cutoff_matrix_",
+    "gpu_upload_calculated_", "gpu_upload_cutoff_", "gpu_get_cshell_eri_", "gpu_delete_",
+    "qk_last_status", "qk_status_string", "qk_set_maxprim", "qk_max_l", "qk_create",
+    "qk_destroy", "qk_default_ctx", "qk_set_basis", "qk_schwarz", "qk_set_schwarz",
+    "qk_set_cutoffs", "qk_fock2e_device", "qk_fock2e_host", "qk_density_cutoff_device",
+    "qk_last_work", "qk_launches_per_build", "qk_oei_host",
+]
+
+_lib = None
+
+
+class QuickError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: status {status} ({status_string(status)})")
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m quick_b200.build` "
+                          f"(or __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    PI = ctypes.POINTER(ctypes.c_int)
+    L.qk_status_string.restype = ctypes.c_char_p
+    L.qk_status_string.argtypes = [I]
+    L.qk_last_status.restype = I
+    L.qk_set_maxprim.argtypes = [I]
+    L.qk_max_l.restype = I
+    L.qk_create.restype = P
+    L.qk_create.argtypes = [I, PI]
+    L.qk_destroy.argtypes = [P]
+    L.qk_default_ctx.restype = P
+    L.qk_set_basis.argtypes = [P, I, P, I, I, I] + [P] * 12 + [I]
+    L.qk_schwarz.argtypes = [P, P, P]
+    L.qk_set_schwarz.argtypes = [P, P, P]
+    L.qk_set_cutoffs.argtypes = [P, D, D]
+    L.qk_fock2e_device.argtypes = [P, P, P, P, P]
+    L.qk_fock2e_host.argtypes = [P, P, P, P]
+    L.qk_density_cutoff_device.argtypes = [P, P, P, P]
+    L.qk_last_work.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), PI]
+    L.qk_launches_per_build.argtypes = [P]
+    L.qk_launches_per_build.restype = I
+    L.qk_oei_host.argtypes = [I, I, P, P, I, I, P, P, P, P, P, I, P, P, P, P, P]
+    L.qk_oei_host.restype = I
+    for name in EXPORTED:
+        if name.startswith("gpu_"):
+            getattr(L, name).restype = None
+    _lib = L
+    return L
+
+
+def status_string(status: int) -> str:
+    try:
+        return lib().qk_status_string(int(status)).decode()
+    except Exception:
+        return "?"
+
+
+def check(status: int, what: str = "quick_b200"):
+    if status != 0:
+        raise QuickError(status, what)

@@ -1,0 +1,305 @@
+"""Generator of the per-class ERI device code (run at build time).
+
+For every shell-quartet class (La Lb | Lc Ld) with La >= Lb, Lc >= Ld and
+La+Lb >= Lc+Ld this script writes straight-line CUDA for
+
+* the Head-Gordon--Pople vertical recursion (HGP eq. 6 and its ket analogue)
+  from F_m(T) to the contracted intermediates [e0|f0], e = La..La+Lb,
+  f = Lc..Lc+Ld (the same recursion QUICK's generated ``iclass_*`` blocks
+  evaluate, ``src/gpu/gpu_eri_assembler_*.h``, ``src/subs/hrr.f90:1051-3456``);
+* the horizontal recursion (a, b+1_i| = (a+1_i, b| + (A-B)_i (a, b| on the bra
+  and the ket (``src/subs/hrr.f90:7-857``);
+* the closed-shell J/K digestion of every integral with QUICK's Cartesian
+  normalisation factors ``cons`` folded in.
+
+Cartesian components follow QUICK's order (``src/basis.f90:589-720``): for a
+total momentum L, z-exponent n ascending, then y-exponent m ascending.
+
+Output: ``generated/eri_classes.cuh`` next to this file.
+"""
+from __future__ import annotations
+
+import itertools
+import math
+import os
+import sys
+
+LMAX = 3  # f shells
+
+
+def carts(L):
+    out = []
+    for n in range(L + 1):
+        for m in range(L + 1 - n):
+            out.append((L - n - m, m, n))
+    return out
+
+
+def ncart(L):
+    return (L + 1) * (L + 2) // 2
+
+
+def cons_of(c):
+    """QUICK normalisation factor of a Cartesian component (src/basis.f90:589-720)."""
+    L = sum(c)
+    if L <= 1:
+        return 1.0
+    nz = sorted([x for x in c if x > 0], reverse=True)
+    if L == 2:
+        return 1.0 if nz == [2] else math.sqrt(3.0)
+    if L == 3:
+        if nz == [3]:
+            return 1.0
+        if nz == [2, 1]:
+            return math.sqrt(5.0)
+        return math.sqrt(5.0) * math.sqrt(3.0)
+    raise ValueError(L)
+
+
+def sub(v, i, k=1):
+    w = list(v)
+    w[i] -= k
+    return tuple(w)
+
+
+def add(v, i, k=1):
+    w = list(v)
+    w[i] += k
+    return tuple(w)
+
+
+ZERO = (0, 0, 0)
+AX = "xyz"
+
+
+class VRRGen:
+    """Builds the VRR DAG for one class and emits code."""
+
+    def __init__(self, Lab, Lcd, e_list, f_list, axis_order):
+        self.Lab, self.Lcd = Lab, Lcd
+        self.order = axis_order
+        self.nodes = {}       # key -> (name, expr)
+        self.emitted = []
+        self.counter = 0
+        self.e_list, self.f_list = e_list, f_list
+
+    def pick(self, v):
+        for i in self.order:
+            if v[i] > 0:
+                return i
+        raise ValueError
+
+    def name(self, e, f, m):
+        key = (e, f, m)
+        if key in self.nodes:
+            return self.nodes[key]
+        if min(e) < 0 or min(f) < 0:
+            return None
+        if e == ZERO and f == ZERO:
+            nm = f"F{m}"
+            self.nodes[key] = nm
+            return nm
+        terms = []
+        if f != ZERO:
+            i = self.pick(f)
+            f1 = sub(f, i)
+            a = self.name(e, f1, m)
+            b = self.name(e, f1, m + 1)
+            terms.append(f"QC{AX[i]} * {a}")
+            terms.append(f"WQ{AX[i]} * {b}")
+            if f1[i] > 0:
+                f2 = sub(f1, i)
+                c = self.name(e, f2, m)
+                d = self.name(e, f2, m + 1)
+                terms.append(f"{float(f1[i])!r} * oo2e * ({c} - rho_e * {d})")
+            if e[i] > 0:
+                em = sub(e, i)
+                g = self.name(em, f1, m + 1)
+                terms.append(f"{float(e[i])!r} * oo2ze * {g}")
+        else:
+            i = self.pick(e)
+            e1 = sub(e, i)
+            a = self.name(e1, ZERO, m)
+            b = self.name(e1, ZERO, m + 1)
+            terms.append(f"PA{AX[i]} * {a}")
+            terms.append(f"WP{AX[i]} * {b}")
+            if e1[i] > 0:
+                e2 = sub(e1, i)
+                c = self.name(e2, ZERO, m)
+                d = self.name(e2, ZERO, m + 1)
+                terms.append(f"{float(e1[i])!r} * oo2z * ({c} - rho_z * {d})")
+        nm = f"v{self.counter}"
+        self.counter += 1
+        self.emitted.append(f"const double {nm} = " + " + ".join(terms) + ";")
+        self.nodes[key] = nm
+        return nm
+
+    def build(self):
+        targets = []
+        for fi, f in enumerate(self.f_list):
+            for ei, e in enumerate(self.e_list):
+                targets.append((fi * len(self.e_list) + ei, self.name(e, f, 0)))
+        return targets
+
+
+def best_vrr(Lab, Lcd, e_list, f_list):
+    best = None
+    for order in itertools.permutations(range(3)):
+        g = VRRGen(Lab, Lcd, e_list, f_list, order)
+        t = g.build()
+        if best is None or g.counter < best[0].counter:
+            best = (g, t)
+    return best
+
+
+def hrr_plan(La, Lb, order=(0, 1, 2)):
+    """Straight-line bra HRR: returns (lines, outputs) where the input column is
+    ``src[idx(e)]`` for e in cart(La..La+Lb) and outputs (a,b) -> expression."""
+    e_list = [c for L in range(La, La + Lb + 1) for c in carts(L)]
+    e_index = {c: k for k, c in enumerate(e_list)}
+    memo = {}
+    lines = []
+    cnt = [0]
+
+    def node(a, b):
+        if (a, b) in memo:
+            return memo[(a, b)]
+        if b == ZERO:
+            nm = f"SRC({e_index[a]})"
+            memo[(a, b)] = nm
+            return nm
+        i = next(k for k in order if b[k] > 0)
+        b1 = sub(b, i)
+        x = node(add(a, i), b1)
+        y = node(a, b1)
+        nm = f"h{cnt[0]}"
+        cnt[0] += 1
+        lines.append(f"const double {nm} = {x} + AB{AX[i]} * {y};")
+        memo[(a, b)] = nm
+        return nm
+
+    outs = []
+    for a in carts(La):
+        for b in carts(Lb):
+            outs.append(node(a, b))
+    return lines, outs, len(e_list)
+
+
+def best_hrr(La, Lb):
+    best = None
+    for order in itertools.permutations(range(3)):
+        r = hrr_plan(La, Lb, order)
+        if best is None or len(r[0]) < len(best[0]):
+            best = r
+    return best
+
+
+def class_list(lmax=LMAX):
+    pcls = [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
+    out = []
+    for (La, Lb) in pcls:
+        for (Lc, Ld) in pcls:
+            if (La + Lb, La, Lb) < (Lc + Ld, Lc, Ld):
+                continue
+            out.append((La, Lb, Lc, Ld))
+    return out
+
+
+def emit_class(La, Lb, Lc, Ld):
+    Lab, Lcd = La + Lb, Lc + Ld
+    M = Lab + Lcd
+    e_list = [c for L in range(La, Lab + 1) for c in carts(L)]
+    f_list = [c for L in range(Lc, Lcd + 1) for c in carts(L)]
+    NE, NF = len(e_list), len(f_list)
+    na, nb, nc, nd = ncart(La), ncart(Lb), ncart(Lc), ncart(Ld)
+    g, targets = best_vrr(Lab, Lcd, e_list, f_list)
+    hb_lines, hb_outs, _ = best_hrr(La, Lb)
+    hk_lines, hk_outs, _ = best_hrr(Lc, Ld)
+    tag = f"{La}{Lb}{Lc}{Ld}"
+    o = []
+    o.append(f"// ---- class ({'spdf'[La]}{'spdf'[Lb]}|{'spdf'[Lc]}{'spdf'[Ld]}): "
+             f"VRR nodes {g.counter}, bra HRR {len(hb_lines)}, ket HRR {len(hk_lines)}")
+    o.append(f"template <> struct EriClass<{La}, {Lb}, {Lc}, {Ld}> {{")
+    o.append(f"  static constexpr int M = {M}, NE = {NE}, NF = {NF};")
+    o.append(f"  static constexpr int NA = {na}, NB = {nb}, NC = {nc}, ND = {nd};")
+    o.append(f"  static constexpr int VRR_NODES = {g.counter}, HRR_BRA = {len(hb_lines)}, HRR_KET = {len(hk_lines)};")
+    # VRR: accumulate acc[f*NE+e] += [e0|f0]^(0) with base F_m already scaled.
+    o.append("  template <typename R>")
+    o.append("  static __device__ __forceinline__ void vrr(const R* __restrict__ Fm, const VrrGeom<R>& G, R* __restrict__ acc) {")
+    o.append("    const R PAx = G.PA[0], PAy = G.PA[1], PAz = G.PA[2];")
+    o.append("    const R WPx = G.WP[0], WPy = G.WP[1], WPz = G.WP[2];")
+    o.append("    const R QCx = G.QC[0], QCy = G.QC[1], QCz = G.QC[2];")
+    o.append("    const R WQx = G.WQ[0], WQy = G.WQ[1], WQz = G.WQ[2];")
+    o.append("    const R oo2z = G.oo2z, oo2e = G.oo2e, oo2ze = G.oo2ze, rho_z = G.rho_z, rho_e = G.rho_e;")
+    o.append("    (void)PAx; (void)PAy; (void)PAz; (void)WPx; (void)WPy; (void)WPz;")
+    o.append("    (void)QCx; (void)QCy; (void)QCz; (void)WQx; (void)WQy; (void)WQz;")
+    o.append("    (void)oo2z; (void)oo2e; (void)oo2ze; (void)rho_z; (void)rho_e;")
+    for m in range(M + 1):
+        o.append(f"    const R F{m} = Fm[{m}];")
+    for ln in g.emitted:
+        o.append("    " + ln.replace("const double", "const R"))
+    for idx, nm in targets:
+        o.append(f"    acc[{idx}] += {nm};")
+    o.append("  }")
+    # bra HRR on one column: SRC(k) = src[k], out[a*NB+b]
+    o.append("  static __device__ __forceinline__ void hrr_bra(const double* __restrict__ src, double* __restrict__ out, double ABx, double ABy, double ABz) {")
+    o.append("    (void)ABx; (void)ABy; (void)ABz;")
+    o.append("#define SRC(k) src[k]")
+    for ln in hb_lines:
+        o.append("    " + ln)
+    for k, nm in enumerate(hb_outs):
+        o.append(f"    out[{k}] = {nm};")
+    o.append("#undef SRC")
+    o.append("  }")
+    # ket HRR on one (ab) row: SRC(k) = src[k*stride]
+    o.append("  static __device__ __forceinline__ void hrr_ket(const double* __restrict__ src, int stride, double* __restrict__ out, double ABx, double ABy, double ABz) {")
+    o.append("    (void)ABx; (void)ABy; (void)ABz;")
+    o.append("#define SRC(k) src[(k) * stride]")
+    for ln in hk_lines:
+        o.append("    " + ln)
+    for k, nm in enumerate(hk_outs):
+        o.append(f"    out[{k}] = {nm};")
+    o.append("#undef SRC")
+    o.append("  }")
+    # cons tables
+    ca = ", ".join(repr(cons_of(c)) for c in carts(La))
+    cb = ", ".join(repr(cons_of(c)) for c in carts(Lb))
+    cc = ", ".join(repr(cons_of(c)) for c in carts(Lc))
+    cd = ", ".join(repr(cons_of(c)) for c in carts(Ld))
+    o.append(f"  static __device__ __forceinline__ double cons_a(int i) {{ const double t[{na}] = {{{ca}}}; return t[i]; }}")
+    o.append(f"  static __device__ __forceinline__ double cons_b(int i) {{ const double t[{nb}] = {{{cb}}}; return t[i]; }}")
+    o.append(f"  static __device__ __forceinline__ double cons_c(int i) {{ const double t[{nc}] = {{{cc}}}; return t[i]; }}")
+    o.append(f"  static __device__ __forceinline__ double cons_d(int i) {{ const double t[{nd}] = {{{cd}}}; return t[i]; }}")
+    o.append("};")
+    stats = dict(cls=tag, vrr=g.counter, hb=len(hb_lines), hk=len(hk_lines), NE=NE, NF=NF)
+    return "\n".join(o), stats
+
+
+def main(out_dir, lmax=LMAX):
+    os.makedirs(out_dir, exist_ok=True)
+    parts = ["// Generated by gen_eri.py -- do not edit.",
+             "#pragma once",
+             "template <int La, int Lb, int Lc, int Ld> struct EriClass;"]
+    stats = []
+    for cls in class_list(lmax):
+        txt, st = emit_class(*cls)
+        parts.append(txt)
+        stats.append(st)
+    # class list for the host
+    parts.append("#define QK_ERI_CLASS_LIST(X) \\")
+    lines = [f"  X({a}, {b}, {c}, {d})" for (a, b, c, d) in class_list(lmax)]
+    parts.append(" \\\n".join(lines))
+    path = os.path.join(out_dir, "eri_classes.cuh")
+    new = "\n".join(parts) + "\n"
+    old = open(path).read() if os.path.exists(path) else None
+    if new != old:
+        with open(path, "w") as f:
+            f.write(new)
+    return stats
+
+
+if __name__ == "__main__":
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.path.dirname(os.path.abspath(__file__)), "generated")
+    lmax = int(sys.argv[2]) if len(sys.argv) > 2 else LMAX
+    for s in main(out, lmax):
+        print(s)

@@ -1,0 +1,225 @@
+"""Host-side interface of the B200 get2e library.
+
+Two faces, both thin layers over ``libquick_b200.so`` (``include/quick_b200.h``):
+
+* :class:`Get2e` -- the context API: one molecule + basis resident on a GPU,
+  Schwarz bounds computed on the device, Fock builds on device tensors
+  (``fock2e``) or host arrays (``fock2e_host``).
+* ``gpu_*`` functions -- the reference's Fortran-to-C call sequence
+  (``src/modules/quick_scf_operator_module.f90:87-127``, ``src/main.f90:152-203``)
+  with the same names, argument order and meaning, passing every argument by
+  reference exactly as gfortran does, so tests read like QUICK's own driver.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import QuickError, check, lib
+
+_c_int = ctypes.c_int
+_c_double = ctypes.c_double
+_c_bool = ctypes.c_bool
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _f64(a):
+    return np.asfortranarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.asfortranarray(a, dtype=np.int32)
+
+
+class Get2e:
+    """One molecule's closed-shell two-electron Fock build on one GPU."""
+
+    def __init__(self, basis, device: int = 0, integral_cutoff: float = 1e-7,
+                 prim_limit: float = 1e-8, schwarz=None):
+        L = lib()
+        st = _c_int(0)
+        self.h = L.qk_create(int(device), ctypes.byref(st))
+        if not self.h:
+            raise QuickError(st.value, "qk_create")
+        self.basis = basis
+        self.device = device
+        b = basis
+        self._keep = [np.ascontiguousarray(b.xyz, dtype=np.float64), _i32(b.kstart), _i32(b.katom),
+                      _i32(b.kprim), _i32(b.ksumtype), _i32(b.qstart), _i32(b.qfinal),
+                      _i32(b.qsbasis), _i32(b.qfbasis), _f64(b.gccoeff), _f64(b.cons),
+                      _f64(b.gcexpo), _i32(b.klmn)]
+        k = self._keep
+        check(L.qk_set_basis(self.h, b.mol.natom, _p(k[0]), b.nshell, b.nbasis, b.jbasis,
+                             *[_p(x) for x in k[1:]], int(b.gccoeff.shape[0])), "qk_set_basis")
+        if schwarz is None:
+            self.Ycut, self.cutprim = self.schwarz()
+        else:
+            self.set_schwarz(*schwarz)
+        self.set_cutoffs(integral_cutoff, prim_limit)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().qk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- per-geometry set-up
+    def schwarz(self):
+        """Ycutoff (nshell^2) and cutprim (jbasis^2) computed on the GPU."""
+        b = self.basis
+        Y = np.zeros((b.nshell, b.nshell), order="F")
+        cp = np.zeros((b.jbasis, b.jbasis), order="F")
+        check(lib().qk_schwarz(self.h, _p(Y), _p(cp)), "qk_schwarz")
+        return Y, cp
+
+    def set_schwarz(self, Y, cutprim):
+        self.Ycut, self.cutprim = _f64(Y), _f64(cutprim)
+        check(lib().qk_set_schwarz(self.h, _p(self.Ycut), _p(self.cutprim)), "qk_set_schwarz")
+
+    def set_cutoffs(self, integral_cutoff: float, prim_limit: float):
+        self.integral_cutoff, self.prim_limit = float(integral_cutoff), float(prim_limit)
+        check(lib().qk_set_cutoffs(self.h, self.integral_cutoff, self.prim_limit), "qk_set_cutoffs")
+
+    # -- Fock builds
+    def fock2e(self, D, o=None, cutmat=None, stream=None):
+        """o += G(D) on the device; D, o, cutmat are CUDA float64 torch tensors.
+
+        Returns o (allocated as zeros when not given).  Enqueued on ``stream``
+        (default: torch's current stream); no synchronisation."""
+        import torch
+        n = self.basis.nbasis
+        if D.dtype != torch.float64 or not D.is_cuda or tuple(D.shape) != (n, n):
+            raise ValueError("D must be a CUDA float64 tensor of shape (nbasis, nbasis)")
+        D = D.contiguous()
+        if o is None:
+            o = torch.zeros((n, n), dtype=torch.float64, device=D.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(D.device)
+        cm = ctypes.c_void_p(cutmat.data_ptr()) if cutmat is not None else None
+        check(lib().qk_fock2e_device(self.h, ctypes.c_void_p(D.data_ptr()), cm,
+                                     ctypes.c_void_p(o.data_ptr()), ctypes.c_void_p(stream.cuda_stream)),
+              "qk_fock2e_device")
+        return o
+
+    def density_cutoff(self, D, out=None, stream=None):
+        import torch
+        ns = self.basis.nshell
+        if out is None:
+            out = torch.empty((ns, ns), dtype=torch.float64, device=D.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(D.device)
+        check(lib().qk_density_cutoff_device(self.h, ctypes.c_void_p(D.data_ptr()),
+                                             ctypes.c_void_p(out.data_ptr()),
+                                             ctypes.c_void_p(stream.cuda_stream)), "qk_density_cutoff_device")
+        return out
+
+    def fock2e_host(self, D, o=None, cutmat=None):
+        """Host arrays: returns o + G(D) (copies in, computes, copies out)."""
+        n = self.basis.nbasis
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        out = np.zeros((n, n)) if o is None else np.array(o, dtype=np.float64, order="C", copy=True)
+        cm = _p(np.ascontiguousarray(cutmat, dtype=np.float64)) if cutmat is not None else None
+        if cutmat is not None:
+            cm_arr = np.ascontiguousarray(cutmat, dtype=np.float64)
+            cm = _p(cm_arr)
+        check(lib().qk_fock2e_host(self.h, _p(D), cm, _p(out)), "qk_fock2e_host")
+        return out
+
+    def work(self):
+        q = ctypes.c_longlong(0)
+        pq = ctypes.c_longlong(0)
+        nl = ctypes.c_int(0)
+        check(lib().qk_last_work(self.h, ctypes.byref(q), ctypes.byref(pq), ctypes.byref(nl)), "qk_last_work")
+        return {"quartets": q.value, "prim_quartets": pq.value, "launches": nl.value}
+
+
+# ---------------------------------------------------------------------------
+# The reference's Fortran -> C call sequence (all arguments by reference).
+# ---------------------------------------------------------------------------
+def _ref(x, ctype):
+    return ctypes.byref(ctype(x))
+
+
+def gpu_new():
+    ierr = _c_int(0)
+    lib().gpu_new_(ctypes.byref(ierr))
+    return ierr.value
+
+
+def gpu_init_device():
+    ierr = _c_int(0)
+    lib().gpu_init_device_(ctypes.byref(ierr))
+    return ierr.value
+
+
+def gpu_setup(natom, nbasis, nelec, imult, molchg, iattype):
+    lib().gpu_setup_(_ref(natom, _c_int), _ref(nbasis, _c_int), _ref(nelec, _c_int),
+                     _ref(imult, _c_int), _ref(molchg, _c_int), _ref(iattype, _c_int))
+
+
+def gpu_upload_method(method=0, is_oshell=False, hyb_coeff=1.0):
+    lib().gpu_upload_method_(_ref(method, _c_int), _ref(is_oshell, _c_bool), _ref(hyb_coeff, _c_double))
+
+
+def gpu_upload_xyz(xyz):
+    x = np.ascontiguousarray(xyz, dtype=np.float64)   # xyz(3, natom) column-major
+    lib().gpu_upload_xyz_(_p(x))
+
+
+def gpu_upload_basis(b):
+    """gpu_upload_basis_ with QUICK's 29 arguments (src/gpu/cuda/gpu.cu:1782)."""
+    z = np.zeros(max(b.mol.natom, b.nshell, 1), dtype=np.int32)
+    args = [
+        _ref(b.nshell, _c_int), _ref(b.nprim, _c_int), _ref(b.nshell, _c_int), _ref(b.jbasis, _c_int),
+        _ref(b.maxcontract, _c_int), _i32(b.ncontract), _i32(b.itype), _f64(b.aexp), _f64(b.dcoeff),
+        z, z, z, z, _i32(b.ncenter), _i32(b.kstart), _i32(b.katom), _i32(b.ktype), _i32(b.kprim),
+        np.zeros(93, dtype=np.int32), _i32(b.ksumtype), _i32(b.qnumber), _i32(b.qstart),
+        _i32(b.qfinal), _i32(b.qsbasis), _i32(b.qfbasis), _f64(b.gccoeff), _f64(b.cons),
+        _f64(b.gcexpo), _i32(b.klmn)]
+    keep = [a for a in args if isinstance(a, np.ndarray)]
+    cargs = [_p(a) if isinstance(a, np.ndarray) else a for a in args]
+    lib().gpu_upload_basis_(*cargs)
+    del keep
+
+
+def gpu_upload_cutoff_matrix(Ycutoff, cutprim):
+    Y, cp = _f64(Ycutoff), _f64(cutprim)
+    lib().gpu_upload_cutoff_matrix_(_p(Y), _p(cp))
+
+
+def gpu_upload_calculated(o, co, vec, dense):
+    o, co, vec, dense = _f64(o), _f64(co), _f64(vec), _f64(dense)
+    lib().gpu_upload_calculated_(_p(o), _p(co), _p(vec), _p(dense))
+
+
+def gpu_upload_cutoff(cutmatrix, integral_cutoff, prim_limit, dm_cutoff=1e-10, core_cutoff=1e-12):
+    cm = _f64(cutmatrix)
+    lib().gpu_upload_cutoff_(_p(cm), _ref(integral_cutoff, _c_double), _ref(prim_limit, _c_double),
+                             _ref(dm_cutoff, _c_double), _ref(core_cutoff, _c_double))
+
+
+def gpu_get_cshell_eri(deltaO, o):
+    """o (Fortran-ordered float64 array) += G(dense); modified in place."""
+    if not (isinstance(o, np.ndarray) and o.dtype == np.float64 and o.flags.f_contiguous):
+        raise ValueError("o must be a Fortran-ordered float64 array")
+    lib().gpu_get_cshell_eri_(_ref(bool(deltaO), _c_bool), _p(o))
+
+
+def gpu_delete():
+    ierr = _c_int(0)
+    lib().gpu_delete_(ctypes.byref(ierr))
+    return ierr.value
+
+
+def last_status():
+    return lib().qk_last_status()
