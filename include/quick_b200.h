@@ -138,6 +138,20 @@ int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int
 /* Kernel launches of one build (for launch accounting). */
 int qk_launches_per_build(qk_ctx *ctx);
 
+/* Per-class measurement: `events` records CUDA events around every class launch on the
+ * launching stream; `stats` counts the quartets and primitive quartets each class
+ * actually evaluated (after density and primitive screening). */
+int qk_set_profiling(qk_ctx *ctx, int events, int stats);
+/* Per-class figures of the last build: cls[4*i] = (La, Lb, Lc, Ld), kernel time in ms,
+ * quartets / primitive quartets listed and evaluated, and the algorithmic FP64
+ * operations per primitive quartet and per quartet.  Returns the number of classes,
+ * or a negative status. */
+int qk_class_profile(qk_ctx *ctx, int max_classes, int *cls, float *ms, long long *q_listed,
+                     long long *pq_listed, long long *q_done, long long *pq_done,
+                     double *prim_flops, double *quartet_flops);
+/* FP64 FMA throughput of device `device` measured by a short probe kernel (GFLOP/s). */
+int qk_fp64_peak(int device, double *gflops);
+
 /* One-electron integrals on device `device` (replaces the get1e path and the
  * reference's gpu_get_oei_, src/gpu/gpu_oei.cu:194; CPU twin
  * src/modules/quick_oei_module.f90:69-257).  Basis in QUICK's normalize_basis

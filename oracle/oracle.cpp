@@ -700,14 +700,17 @@ void orc_density_cutoff(void* hv, const double* dense, double* cutmatrix) {
 }
 
 // o += G(dense) for the screened quartet set; returns the number of shell
-// quartets evaluated.  Shells II in [ii_begin, ii_end) only (a bounded sample
-// when the range is partial).  nthreads <= 0 uses the OpenMP default.
+// quartets evaluated.  Bra shells II = ii_begin, ii_begin + ii_stride, ... < ii_end
+// only (a bounded sample when the range is partial).  nthreads <= 0 uses the
+// OpenMP default.
 long long orc_get2e(void* hv, const double* dense, const double* cutmatrix, const double* Ycutoff,
                     const double* cutprim, double integralCutoff, double primLimit, double* o,
-                    int ii_begin, int ii_end, int nthreads) {
+                    int ii_begin, int ii_end, int nthreads, int ii_stride) {
     Basis& B = ((OracleHandle*)hv)->B;
     int n = B.nbasis, ns = B.nshell;
     if (ii_end <= 0 || ii_end > ns) ii_end = ns;
+    if (ii_stride <= 0) ii_stride = 1;
+    const int nII = (ii_end - ii_begin + ii_stride - 1) / ii_stride;
     Ctx C{&B, dense, cutmatrix, cutprim, integralCutoff, primLimit};
     std::vector<double> G((size_t)n * n, 0.0);
     long long nq = 0;
@@ -719,7 +722,8 @@ long long orc_get2e(void* hv, const double* dense, const double* cutmatrix, cons
         Work W;
         std::vector<double> Gt((size_t)n * n, 0.0);
 #pragma omp for schedule(dynamic, 1) nowait
-        for (int II = ii_begin; II < ii_end; ++II)
+        for (int t = 0; t < nII; ++t) {
+            const int II = ii_begin + t * ii_stride;
             for (int JJ = II; JJ < ns; ++JJ) {
                 double t = Ycutoff[II + (size_t)ns * JJ];
                 for (int KK = II; KK < ns; ++KK)
@@ -732,6 +736,7 @@ long long orc_get2e(void* hv, const double* dense, const double* cutmatrix, cons
                         ++nq;
                     }
             }
+        }
 #pragma omp critical
         for (size_t i = 0; i < G.size(); ++i) G[i] += Gt[i];
     }

@@ -20,7 +20,8 @@ EXPORTED = [
     "qk_last_status", "qk_status_string", "qk_set_maxprim", "qk_max_l", "qk_create",
     "qk_destroy", "qk_default_ctx", "qk_set_basis", "qk_schwarz", "qk_set_schwarz",
     "qk_set_cutoffs", "qk_fock2e_device", "qk_fock2e_host", "qk_density_cutoff_device",
-    "qk_last_work", "qk_launches_per_build", "qk_oei_host",
+    "qk_last_work", "qk_launches_per_build", "qk_oei_host", "qk_set_profiling",
+    "qk_class_profile", "qk_fp64_peak",
 ]
 
 _lib = None
@@ -63,6 +64,10 @@ def lib():
     L.qk_launches_per_build.restype = I
     L.qk_oei_host.argtypes = [I, I, P, P, I, I, P, P, P, P, P, I, P, P, P, P, P]
     L.qk_oei_host.restype = I
+    L.qk_set_profiling.argtypes = [P, I, I]
+    L.qk_class_profile.argtypes = [P, I, P, P, P, P, P, P, P, P]
+    L.qk_class_profile.restype = I
+    L.qk_fp64_peak.argtypes = [I, ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED:
         if name.startswith("gpu_"):
             getattr(L, name).restype = None

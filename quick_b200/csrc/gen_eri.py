@@ -223,6 +223,8 @@ def emit_class(La, Lb, Lc, Ld):
     o.append(f"  static constexpr int M = {M}, NE = {NE}, NF = {NF};")
     o.append(f"  static constexpr int NA = {na}, NB = {nb}, NC = {nc}, ND = {nd};")
     o.append(f"  static constexpr int VRR_NODES = {g.counter}, HRR_BRA = {len(hb_lines)}, HRR_KET = {len(hk_lines)};")
+    pf, qf = class_flops(La, Lb, Lc, Ld)
+    o.append(f"  static constexpr double PRIM_FLOPS = {pf}.0, QUARTET_FLOPS = {qf}.0;")
     # VRR: accumulate acc[f*NE+e] += [e0|f0]^(0) with base F_m already scaled.
     o.append("  template <typename R>")
     o.append("  static __device__ __forceinline__ void vrr(const R* __restrict__ Fm, const VrrGeom<R>& G, R* __restrict__ acc) {")
@@ -273,6 +275,38 @@ def emit_class(La, Lb, Lc, Ld):
     o.append("};")
     stats = dict(cls=tag, vrr=g.counter, hb=len(hb_lines), hk=len(hk_lines), NE=NE, NF=NF)
     return "\n".join(o), stats
+
+
+def count_flops(expr_lines):
+    """FP operations in emitted expressions: every binary * + - counts 1."""
+    n = 0
+    for ln in expr_lines:
+        rhs = ln.split("=", 1)[1]
+        n += rhs.count("*") + rhs.count(" + ") + rhs.count(" - ")
+    return n
+
+
+def boys_flops(M):
+    # 7-term Taylor (7 mul + 6 fma = 19) plus, for M > 0, exp (1) and 3 per downward step;
+    # scaling by the prefactor 1 per m
+    return 19 + (1 + 3 * M if M > 0 else 0) + (M + 1)
+
+
+def class_flops(La, Lb, Lc, Ld):
+    """Algorithmic FP64 operation counts of one class: per primitive quartet and per
+    contracted quartet (the model the benchmark's roofline uses)."""
+    Lab, Lcd = La + Lb, Lc + Ld
+    e_list = [c for L in range(La, Lab + 1) for c in carts(L)]
+    f_list = [c for L in range(Lc, Lcd + 1) for c in carts(L)]
+    g, _ = best_vrr(Lab, Lcd, e_list, f_list)
+    hb, _, _ = best_hrr(La, Lb)
+    hk, _, _ = best_hrr(Lc, Ld)
+    NE, NF = len(e_list), len(f_list)
+    na, nb, nc, nd = ncart(La), ncart(Lb), ncart(Lc), ncart(Ld)
+    geom = 30   # zeta+eta, 1/(zeta+eta), rho, PQ, T, prefactor (div, sqrt counted 1 each), W-P, W-Q
+    prim = geom + boys_flops(Lab + Lcd) + count_flops(g.emitted) + NE * NF
+    quartet = NF * 2 * len(hb) + na * nb * 2 * len(hk) + na * nb * nc * nd * 13
+    return prim, quartet
 
 
 def main(out_dir, lmax=LMAX):

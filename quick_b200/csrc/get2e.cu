@@ -63,6 +63,7 @@ struct DevData {
     const double* __restrict__ D;        // nbasis^2
     const double* __restrict__ cutmat;   // nshell^2
     unsigned long long* __restrict__ A;  // nbasis^2 fixed point
+    unsigned long long* stats;           // optional: [quartets computed, primitive quartets computed]
     double cut, primLimit;
 };
 
@@ -82,7 +83,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 template <int La, int Lb, int Lc, int Ld>
 __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int bnp, int kp0, int knp,
                                                  const double C[3], double dnmax, bool prim_screen,
-                                                 double* acc) {
+                                                 double* acc, int* nprim_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int M = Cls::M;
 #pragma unroll
@@ -98,6 +99,7 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
         for (int j = 0; j < knp; ++j) {
             const int pj = kp0 + j;
             if (prim_screen && !(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;
+            ++*nprim_done;
             const double eta = __ldg(d.pp_zeta + pj);
             const double Qx = __ldg(d.pp_P + 3 * pj), Qy = __ldg(d.pp_P + 3 * pj + 1), Qz = __ldg(d.pp_P + 3 * pj + 2);
             const double s = zeta + eta;
@@ -128,7 +130,8 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
 // Lane-private updates go straight to A; the bra J block is returned in jab
 // (already weighted) for the warp reduction.
 template <int La, int Lb, int Lc, int Ld>
-__device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, double* jab_out) {
+__device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, double* jab_out, int* nq_done,
+                                             int* np_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND;
     constexpr int NE = Cls::NE, NF = Cls::NF, NAB = NA * NB;
@@ -141,6 +144,7 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, dou
     dnmax = fmax(dnmax, fmax(cm[sb * ns + sc], cm[sb * ns + sd]));
     const double ct = d.pr_Y[P] * d.pr_Y[Q];
     if (!(ct * dnmax > d.cut)) return;
+    ++*nq_done;
 
     const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
     const double AB[3] = {d.xyz[3 * ia] - d.xyz[3 * ib], d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
@@ -149,7 +153,8 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, dou
     const double CD[3] = {Cc[0] - d.xyz[3 * id], Cc[1] - d.xyz[3 * id + 1], Cc[2] - d.xyz[3 * id + 2]};
 
     double acc[NE * NF];
-    contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pp0[Q], d.pr_npp[Q], Cc, dnmax, true, acc);
+    contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pp0[Q], d.pr_npp[Q], Cc, dnmax, true, acc,
+                                     np_done);
 
     // bra HRR per ket column
     double t1[NF * NAB];
@@ -264,7 +269,16 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
         double jab[NAB];
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, jab);
+        int nq = 0, np = 0;
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, jab, &nq, &np);
+        if (d.stats) {
+            const unsigned sq = __reduce_add_sync(0xffffffffu, (unsigned)nq);
+            const unsigned sp = __reduce_add_sync(0xffffffffu, (unsigned)np);
+            if (lane == 0) {
+                atomicAdd(d.stats, (unsigned long long)sq);
+                atomicAdd(d.stats + 1, (unsigned long long)sp);
+            }
+        }
         const int P = w.x;
         const int qa = d.pr_qa[P], qb = d.pr_qb[P];
         const int fa = d.q_f0[qa], fb = d.q_f0[qb];
@@ -300,7 +314,8 @@ schwarz_kernel(DevData d, const int2* __restrict__ work, int n_work, const int* 
     int p0 = d.pr_pp0[P], np = d.pr_npp[P];
     if (mode >= 0) { p0 += mode; np = 1; }
     double acc[NE * NF];
-    contract_quartet<La, Lb, La, Lb>(d, p0, np, p0, np, Cc, 0.0, false, acc);
+    int ndone = 0;
+    contract_quartet<La, Lb, La, Lb>(d, p0, np, p0, np, Cc, 0.0, false, acc, &ndone);
     double t1[NF * NAB];
 #pragma unroll
     for (int f = 0; f < NF; ++f) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, AB[0], AB[1], AB[2]);
@@ -342,6 +357,21 @@ __global__ void density_cutoff_kernel(const double* __restrict__ D, int n, int n
     for (int i = s_f0[a]; i < s_f1[a]; ++i)
         for (int j = s_f0[b]; j < s_f1[b]; ++j) m = fmax(m, fabs(D[(size_t)j * n + i]));
     cutmat[t] = m;
+}
+
+// FP64 FMA throughput probe: independent dependent-chains per thread.
+__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+    double x0 = threadIdx.x * 1e-3, x1 = x0 + 1.0, x2 = x0 + 2.0, x3 = x0 + 3.0;
+    double x4 = x0 + 4.0, x5 = x0 + 5.0, x6 = x0 + 6.0, x7 = x0 + 7.0;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    const double r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (r == 12345.678) out[0] = r;   // keeps the chains live
 }
 
 __global__ void finalize_kernel(const unsigned long long* __restrict__ A, int n, double* __restrict__ o) {
@@ -419,8 +449,10 @@ struct ClassEntry {
     int La, Lb, Lc, Ld;
     FockFn fn;
     const void* (*kernel)();
+    double prim_flops, quartet_flops;   // algorithmic FP64 operations (gen_eri.py model)
 };
-#define QK_X(a, b, c, e) {a, b, c, e, &launch_fock<a, b, c, e>, &fock_fn_ptr<a, b, c, e>},
+#define QK_X(a, b, c, e) {a, b, c, e, &launch_fock<a, b, c, e>, &fock_fn_ptr<a, b, c, e>, \
+                          EriClass<a, b, c, e>::PRIM_FLOPS, EriClass<a, b, c, e>::QUARTET_FLOPS},
 static const ClassEntry g_classes[] = {QK_ERI_CLASS_LIST(QK_X)};
 #undef QK_X
 constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
@@ -458,6 +490,11 @@ struct qk_ctx {
     qk::DevBuf<int> d_q_atom, d_q_f0, d_q_parent, d_q_prim0, d_q_nprim, d_shell_f0, d_shell_f1;
     qk::DevBuf<unsigned long long> d_A;
     qk::DevBuf<int> d_counters;
+    // optional per-class timing (CUDA events on the launching stream) and work counters
+    bool profile_events = false, profile_stats = false;
+    cudaEvent_t ev[2 * qk::kNumClasses] = {};
+    bool ev_recorded[qk::kNumClasses] = {};
+    qk::DevBuf<unsigned long long> d_stats;
     // drop-in (reference-shaped) state
     std::vector<double> host_D, host_cutmat;
     bool have_D = false, have_cutmat = false;
@@ -715,13 +752,25 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     d.D = D;
     d.cutmat = cutmat;
     d.A = c->d_A.p;
+    d.stats = nullptr;
+    if (c->profile_stats) {
+        QK_CUDA_TRY(c->d_stats.reserve(2 * kNumClasses));
+        QK_CUDA_TRY(cudaMemsetAsync(c->d_stats.p, 0, sizeof(unsigned long long) * 2 * kNumClasses, s));
+    }
     long long nq = 0, npq = 0;
     for (int ci = 0; ci < kNumClasses; ++ci) {
         ClassWork& W = c->work[ci];
+        c->ev_recorded[ci] = false;
         if (W.items.empty()) continue;
+        if (c->profile_stats) d.stats = c->d_stats.p + 2 * ci;
+        if (c->profile_events) QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci], s));
         g_classes[ci].fn(dim3(W.grid), dim3(32 * kWarpsPerBlock), s, d, W.d_items.p, (int)W.items.size(),
                          c->d_counters.p + ci);
         QK_CUDA_TRY(cudaGetLastError());
+        if (c->profile_events) {
+            QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci + 1], s));
+            c->ev_recorded[ci] = true;
+        }
         nq += W.nquart;
         npq += W.nprimq;
     }
@@ -802,6 +851,8 @@ int qk_destroy(qk_ctx* c) {
     if (!c) return QK_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
     delete c;
     return QK_OK;
@@ -1035,6 +1086,80 @@ int qk_last_work(qk_ctx* c, long long* quartets, long long* primq, int* launches
 }
 
 int qk_launches_per_build(qk_ctx* c) { return c ? c->launches : 0; }
+
+int qk_set_profiling(qk_ctx* c, int events, int stats) {
+    if (!c) return fail(QK_ERR_INVALID_ARG, "null context");
+    std::lock_guard<std::mutex> g(c->mu);
+    cudaSetDevice(c->device);
+    if (events && !c->ev[0])
+        for (auto& e : c->ev) QK_CUDA_TRY(cudaEventCreate(&e));
+    c->profile_events = events != 0;
+    c->profile_stats = stats != 0;
+    return QK_OK;
+}
+
+int qk_class_profile(qk_ctx* c, int max_classes, int* cls, float* ms, long long* q_listed,
+                     long long* pq_listed, long long* q_done, long long* pq_done, double* prim_flops,
+                     double* quartet_flops) {
+    if (!c) return -fail(QK_ERR_INVALID_ARG, "null context");
+    std::lock_guard<std::mutex> g(c->mu);
+    cudaSetDevice(c->device);
+    std::vector<unsigned long long> st(2 * kNumClasses, 0);
+    if (c->profile_stats && c->d_stats.p) {
+        if (cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(st.data(), c->d_stats.p, st.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return -fail(QK_ERR_CUDA, "stats download");
+    }
+    const int n = std::min(max_classes, kNumClasses);
+    for (int i = 0; i < n; ++i) {
+        const ClassEntry& ce = g_classes[i];
+        if (cls) { cls[4 * i] = ce.La; cls[4 * i + 1] = ce.Lb; cls[4 * i + 2] = ce.Lc; cls[4 * i + 3] = ce.Ld; }
+        float t = 0.0f;
+        if (c->profile_events && c->ev_recorded[i]) {
+            if (cudaEventSynchronize(c->ev[2 * i + 1]) != cudaSuccess ||
+                cudaEventElapsedTime(&t, c->ev[2 * i], c->ev[2 * i + 1]) != cudaSuccess)
+                return -fail(QK_ERR_CUDA, "event timing");
+        }
+        if (ms) ms[i] = t;
+        if (q_listed) q_listed[i] = c->work[i].nquart;
+        if (pq_listed) pq_listed[i] = c->work[i].nprimq;
+        if (q_done) q_done[i] = (long long)st[2 * i];
+        if (pq_done) pq_done[i] = (long long)st[2 * i + 1];
+        if (prim_flops) prim_flops[i] = ce.prim_flops;
+        if (quartet_flops) quartet_flops[i] = ce.quartet_flops;
+    }
+    return n;
+}
+
+int qk_fp64_peak(int device, double* gflops) {
+    if (!gflops) return fail(QK_ERR_INVALID_ARG, "null output");
+    if (cudaSetDevice(device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    DevBuf<double> out;
+    QK_CUDA_TRY(out.reserve(1));
+    cudaEvent_t e0, e1;
+    QK_CUDA_TRY(cudaEventCreate(&e0));
+    QK_CUDA_TRY(cudaEventCreate(&e1));
+    const int blocks = sms * 8, threads = 256, iters = 2000;
+    fp64_probe_kernel<<<blocks, threads>>>(out.p, 200, 0.999999, 1e-7);   // warm-up
+    QK_CUDA_TRY(cudaGetLastError());
+    float best = 1e30f;
+    for (int r = 0; r < 5; ++r) {
+        QK_CUDA_TRY(cudaEventRecord(e0));
+        fp64_probe_kernel<<<blocks, threads>>>(out.p, iters, 0.999999, 1e-7);
+        QK_CUDA_TRY(cudaEventRecord(e1));
+        QK_CUDA_TRY(cudaEventSynchronize(e1));
+        float t = 0.0f;
+        QK_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+        best = std::min(best, t);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    *gflops = flops / (best * 1e-3) * 1e-9;
+    return QK_OK;
+}
 
 // ------------------------------------------------------------- drop-in layer
 void gpu_new_(int* ierr) {

@@ -1,0 +1,52 @@
+"""GPU one-electron integrals and the SCF driver built on the B200 Fock build."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from quick_b200.basis import Molecule, build_basis  # noqa: E402
+from quick_b200.molecules import water_cluster  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def water():
+    return Molecule.from_angstrom(["O", "H", "H"], [[-0.3384, 0.0038, 0.23923], [-0.3351, -0.0019, -0.83277],
+                                                   [0.6735, -0.0019, 0.59353]])
+
+
+@pytest.mark.parametrize("bas", ["STO-3G", "6-31G*", "CC-PVDZ"])
+def test_oei_matches_oracle(bas):
+    _cuda()
+    from quick_b200.scf import oei
+    b = build_basis(water_cluster(2, 5.0), bas)
+    rng = np.random.default_rng(1)
+    ext = (rng.uniform(-8, 8, size=(20, 3)), rng.uniform(-0.8, 0.8, size=20))
+    S, T, V = oei(b, ext)
+    S0, T0, V0 = O.oei(b, ext)
+    for x, y in ((S, S0), (T, T0), (V, V0)):
+        assert np.abs(x - y).max() <= 1e-10 * max(1.0, np.abs(y).max())
+
+
+def test_rhf_energy_golden_h2o_631gs():
+    _cuda()
+    from quick_b200.scf import RHF
+    b = build_basis(water(), "6-31G*")
+    r = RHF(b, integral_cutoff=1e-11).run(denserms=1e-8)
+    assert r["converged"]
+    assert abs(r["E"] - (-75.983996360)) <= 1e-6
+
+
+def test_rhf_matches_oracle_w4_sto3g():
+    _cuda()
+    from quick_b200.scf import RHF
+    b = build_basis(water_cluster(4, 6.0), "STO-3G")
+    ref = O.rhf(b, guess="gwh", integral_cutoff=1e-10, prim_limit=1e-11)
+    r = RHF(b, integral_cutoff=1e-10).run(denserms=1e-8)
+    assert r["converged"]
+    assert abs(r["E"] - ref["E"]) <= 1e-7, (r["E"], ref["E"])
