@@ -47,7 +47,14 @@ __device__ __forceinline__ void boys_scaled(double T, double scale, const double
         if (M == 0) {
             F[0] = f * scale;
         } else {
-            const double e = exp(-T);
+            // exp(-T) = exp(-T_k) * exp(u), exp(u) by its 7-term series (|u| <= 0.025)
+            double eu = fma(u, 1.0 / 720.0, 1.0 / 120.0);
+            eu = fma(eu, u, 1.0 / 24.0);
+            eu = fma(eu, u, 1.0 / 6.0);
+            eu = fma(eu, u, 0.5);
+            eu = fma(eu, u, 1.0);
+            eu = fma(eu, u, 1.0);
+            const double e = __ldg(tab + kBoysNT * kBoysNM + k) * eu;
             const double T2 = 2.0 * T;
             double fm = f;
             F[M] = fm * scale;
@@ -89,6 +96,8 @@ inline std::vector<double> boys_table() {
             t[(size_t)k * kBoysNM + m] = (double)(expl(-T) * sum);
         }
     }
+    // exp(-T_k) after the table (used for the downward recursion)
+    for (int k = 0; k < kBoysNT; ++k) t.push_back((double)expl(-(long double)k * kBoysDT));
     return t;
 }
 

@@ -82,6 +82,8 @@ class VRRGen:
         self.emitted = []
         self.counter = 0
         self.e_list, self.f_list = e_list, f_list
+        self.struct = []      # (name, key, record) in creation (topological) order
+        self._last = None
 
     def pick(self, v):
         for i in self.order:
@@ -100,38 +102,50 @@ class VRRGen:
             self.nodes[key] = nm
             return nm
         terms = []
+        # structural record: (kind, axis, a, b, c, d, g, n2, na) with operand names or None
         if f != ZERO:
             i = self.pick(f)
             f1 = sub(f, i)
             a = self.name(e, f1, m)
             b = self.name(e, f1, m + 1)
+            c = d = g = None
+            n2 = na = 0.0
             terms.append(f"QC{AX[i]} * {a}")
             terms.append(f"WQ{AX[i]} * {b}")
             if f1[i] > 0:
                 f2 = sub(f1, i)
                 c = self.name(e, f2, m)
                 d = self.name(e, f2, m + 1)
+                n2 = float(f1[i])
                 terms.append(f"{float(f1[i])!r} * oo2e * ({c} - rho_e * {d})")
             if e[i] > 0:
                 em = sub(e, i)
                 g = self.name(em, f1, m + 1)
+                na = float(e[i])
                 terms.append(f"{float(e[i])!r} * oo2ze * {g}")
+            rec = (1, i, a, b, c, d, g, n2, na)
         else:
             i = self.pick(e)
             e1 = sub(e, i)
             a = self.name(e1, ZERO, m)
             b = self.name(e1, ZERO, m + 1)
+            c = d = None
+            n2 = 0.0
             terms.append(f"PA{AX[i]} * {a}")
             terms.append(f"WP{AX[i]} * {b}")
             if e1[i] > 0:
                 e2 = sub(e1, i)
                 c = self.name(e2, ZERO, m)
                 d = self.name(e2, ZERO, m + 1)
+                n2 = float(e1[i])
                 terms.append(f"{float(e1[i])!r} * oo2z * ({c} - rho_z * {d})")
+            rec = (0, i, a, b, c, d, None, n2, 0.0)
+        self._last = rec
         nm = f"v{self.counter}"
         self.counter += 1
         self.emitted.append(f"const double {nm} = " + " + ".join(terms) + ";")
         self.nodes[key] = nm
+        self.struct.append((nm, key, self._last))
         return nm
 
     def build(self):
@@ -192,6 +206,36 @@ def best_hrr(La, Lb):
         if best is None or len(r[0]) < len(best[0]):
             best = r
     return best
+
+
+COOP_MIN = 150   # NE*NF at or above which a class uses the warp-cooperative kernel
+
+
+def vrr_table(g, targets, M):
+    """Level-ordered node table for the warp-cooperative VRR.
+
+    Slot layout of the per-warp value array V: 0..M = scaled F_m, M+1 = 0.0,
+    M+2+k = node k in level order.  Returns (rows, level_offsets, target_slots)."""
+    level = {f"F{m}": 0 for m in range(M + 1)}
+    for nm, key, rec in g.struct:
+        ops = [x for x in rec[2:7] if x is not None]
+        level[nm] = 1 + max(level[x] for x in ops)
+    order = sorted(g.struct, key=lambda t: (level[t[0]], int(t[0][1:])))
+    slot = {f"F{m}": m for m in range(M + 1)}
+    for k, (nm, _, _) in enumerate(order):
+        slot[nm] = M + 2 + k
+    zero = M + 1
+    rows = []
+    for nm, key, rec in order:
+        kind, axis, a, b, c, d, gg, n2, na = rec
+        sl = lambda x: slot[x] if x is not None else zero  # noqa: E731
+        rows.append((kind, axis, sl(a), sl(b), sl(c), sl(d), sl(gg), n2, na))
+    nlev = max(level.values())
+    off = [0]
+    for L in range(1, nlev + 1):
+        off.append(off[-1] + sum(1 for t in order if level[t[0]] == L))
+    tslots = [slot[nm] for _, nm in sorted(targets)]
+    return rows, off, tslots
 
 
 def class_list(lmax=LMAX):
@@ -272,8 +316,22 @@ def emit_class(La, Lb, Lc, Ld):
     o.append(f"  static __device__ __forceinline__ double cons_b(int i) {{ const double t[{nb}] = {{{cb}}}; return t[i]; }}")
     o.append(f"  static __device__ __forceinline__ double cons_c(int i) {{ const double t[{nc}] = {{{cc}}}; return t[i]; }}")
     o.append(f"  static __device__ __forceinline__ double cons_d(int i) {{ const double t[{nd}] = {{{cd}}}; return t[i]; }}")
+    coop = NE * NF >= COOP_MIN
+    o.append(f"  static constexpr bool COOP = {'true' if coop else 'false'};")
+    if coop:
+        rows, off, tslots = vrr_table(g, targets, M)
+        o.append(f"  static constexpr int NNODE = {len(rows)}, NLEVEL = {len(off) - 1}, NSLOT = {M + 2 + len(rows)};")
+        o.append(f"  static __device__ const VrrNode* nodes() {{ return vrr_nodes_{tag}; }}")
+        o.append(f"  static __device__ const short* level_off() {{ return vrr_levels_{tag}; }}")
+        o.append(f"  static __device__ const short* targets() {{ return vrr_targets_{tag}; }}")
+        tab = ",\n".join(f"  {{{k}, {a}, {x}, {y}, {z}, {w}, {v}, {n2!r}f, {na!r}f}}"
+                          for (k, a, x, y, z, w, v, n2, na) in rows)
+        pre = [f"__device__ const VrrNode vrr_nodes_{tag}[{len(rows)}] = {{\n{tab}\n}};",
+               f"__device__ const short vrr_levels_{tag}[{len(off)}] = {{{', '.join(map(str, off))}}};",
+               f"__device__ const short vrr_targets_{tag}[{len(tslots)}] = {{{', '.join(map(str, tslots))}}};"]
+        o = o[:1] + pre + o[1:]
     o.append("};")
-    stats = dict(cls=tag, vrr=g.counter, hb=len(hb_lines), hk=len(hk_lines), NE=NE, NF=NF)
+    stats = dict(cls=tag, vrr=g.counter, hb=len(hb_lines), hk=len(hk_lines), NE=NE, NF=NF, coop=coop)
     return "\n".join(o), stats
 
 
@@ -313,6 +371,8 @@ def main(out_dir, lmax=LMAX):
     os.makedirs(out_dir, exist_ok=True)
     parts = ["// Generated by gen_eri.py -- do not edit.",
              "#pragma once",
+             "// one VRR node: kind 0 = bra step (PA, WP, oo2z, rho_z), 1 = ket step (QC, WQ, oo2e, rho_e)",
+             "struct VrrNode { unsigned char kind, axis; short a, b, c, d, g; float n2, na; };",
              "template <int La, int Lb, int Lc, int Ld> struct EriClass;"]
     stats = []
     for cls in class_list(lmax):

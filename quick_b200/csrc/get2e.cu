@@ -52,13 +52,18 @@ struct DevData {
     const int* __restrict__ pr_qb;
     const int* __restrict__ pr_pp0;
     const int* __restrict__ pr_npp;
+    const int* __restrict__ pr_pps;      // stride between a pair's primitive pairs
     const double* __restrict__ pr_Y;
     const double* __restrict__ pp_zeta;  // per primitive pair
     const double* __restrict__ pp_oo2z;
     const double* __restrict__ pp_K;
     const double* __restrict__ pp_cut;
-    const double* __restrict__ pp_P;     // 3 per primitive pair
-    const double* __restrict__ pp_PA;    // 3 per primitive pair (P - centre of first shell)
+    const double* __restrict__ pp_Px;    // P, and P - centre of the first shell
+    const double* __restrict__ pp_Py;
+    const double* __restrict__ pp_Pz;
+    const double* __restrict__ pp_PAx;
+    const double* __restrict__ pp_PAy;
+    const double* __restrict__ pp_PAz;
     const double* __restrict__ boys;     // kBoysNT x kBoysNM
     const double* __restrict__ D;        // nbasis^2
     const double* __restrict__ cutmat;   // nshell^2
@@ -81,7 +86,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Contracted [e0|f0] over the primitive pairs of a bra and a ket pair.
 // acc[f*NE + e]; prim_screen applies QUICK's primitive cutoff.
 template <int La, int Lb, int Lc, int Ld>
-__device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int bnp, int kp0, int knp,
+__device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int bnp, int bps, int kp0, int knp,
+                                                 int kps,
                                                  const double C[3], double dnmax, bool prim_screen,
                                                  double* acc, int* nprim_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
@@ -89,26 +95,27 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
 #pragma unroll
     for (int i = 0; i < Cls::NE * Cls::NF; ++i) acc[i] = 0.0;
     for (int i = 0; i < bnp; ++i) {
-        const int pi = bp0 + i;
+        const int pi = bp0 + i * bps;
         const double zeta = __ldg(d.pp_zeta + pi);
         const double oo2z = __ldg(d.pp_oo2z + pi);
         const double Kab = __ldg(d.pp_K + pi) * kX0;
         const double cut1 = dnmax * __ldg(d.pp_cut + pi);
-        const double Px = __ldg(d.pp_P + 3 * pi), Py = __ldg(d.pp_P + 3 * pi + 1), Pz = __ldg(d.pp_P + 3 * pi + 2);
-        const double PAx = __ldg(d.pp_PA + 3 * pi), PAy = __ldg(d.pp_PA + 3 * pi + 1), PAz = __ldg(d.pp_PA + 3 * pi + 2);
+        const double Px = __ldg(d.pp_Px + pi), Py = __ldg(d.pp_Py + pi), Pz = __ldg(d.pp_Pz + pi);
+        const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
         for (int j = 0; j < knp; ++j) {
-            const int pj = kp0 + j;
+            const int pj = kp0 + j * kps;
             if (prim_screen && !(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;
             ++*nprim_done;
             const double eta = __ldg(d.pp_zeta + pj);
-            const double Qx = __ldg(d.pp_P + 3 * pj), Qy = __ldg(d.pp_P + 3 * pj + 1), Qz = __ldg(d.pp_P + 3 * pj + 2);
+            const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
             const double s = zeta + eta;
-            const double inv_s = 1.0 / s;
+            const double rs = rsqrt(s);            // 1/sqrt(zeta+eta), 1 ulp
+            const double inv_s = rs * rs;
             const double rho_z = eta * inv_s, rho_e = zeta * inv_s;
             const double rho = zeta * rho_z;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = Kab * __ldg(d.pp_K + pj) * sqrt(inv_s);
+            const double pref = Kab * __ldg(d.pp_K + pj) * rs;
             double F[M + 1];
             boys_scaled<M>(T, pref, d.boys, F);
             VrrGeom<double> G;
@@ -153,8 +160,8 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, dou
     const double CD[3] = {Cc[0] - d.xyz[3 * id], Cc[1] - d.xyz[3 * id + 1], Cc[2] - d.xyz[3 * id + 2]};
 
     double acc[NE * NF];
-    contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pp0[Q], d.pr_npp[Q], Cc, dnmax, true, acc,
-                                     np_done);
+    contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q],
+                                     d.pr_pps[Q], Cc, dnmax, true, acc, np_done);
 
     // bra HRR per ket column
     double t1[NF * NAB];
@@ -253,6 +260,220 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, dou
         for (int e = 0; e < ND; ++e) atomic_fixed(A + (size_t)(fb + b) * n + fd + e, wK * kbd[b * ND + e]);
 }
 
+// ------------------------------------------------------------------ warp-cooperative classes
+// High angular momentum classes (NE*NF >= 150) evaluate ONE quartet per warp:
+// the VRR runs as a level-ordered node table over the 32 lanes with the values in
+// shared memory, the bra HRR runs one ket column per lane, the ket HRR one bra
+// row per lane, and the digestion one output element per lane (a fixed-order dot
+// product, so results stay deterministic).
+
+// F_m(T) for one m (lane-parallel Boys): Taylor on the grid, or upward recursion
+// from the asymptotic F_0 above the grid.
+__device__ __forceinline__ double boys_one(int m, double T, const double* __restrict__ tab) {
+    if (T < kBoysTmax) {
+        const int k = __double2int_rn(T * kBoysInvDT);
+        const double u = k * kBoysDT - T;
+        const double* t = tab + k * kBoysNM + m;
+        double f = __ldg(t + 6) * (1.0 / 720.0);
+        f = fma(f, u, __ldg(t + 5) * (1.0 / 120.0));
+        f = fma(f, u, __ldg(t + 4) * (1.0 / 24.0));
+        f = fma(f, u, __ldg(t + 3) * (1.0 / 6.0));
+        f = fma(f, u, __ldg(t + 2) * 0.5);
+        f = fma(f, u, __ldg(t + 1));
+        return fma(f, u, __ldg(t + 0));
+    }
+    double f = kHalfSqrtPi * rsqrt(T);
+    if (m > 0) {
+        const double e = exp(-T), h = 0.5 / T;
+        for (int j = 0; j < m; ++j) f = fma((double)(2 * j + 1), f, -e) * h;
+    }
+    return f;
+}
+
+template <int La, int Lb, int Lc, int Ld>
+struct CoopLayout {
+    using Cls = EriClass<La, Lb, Lc, Ld>;
+    static constexpr int NAB = Cls::NA * Cls::NB, NCD = Cls::NC * Cls::ND;
+    static constexpr int ACC = Cls::NE * Cls::NF;
+    static constexpr int HRR = Cls::NF * NAB + NAB * NCD;
+    static constexpr int WORK = Cls::NSLOT > HRR ? Cls::NSLOT : HRR;
+    static constexpr int DBLK = NAB + NCD + Cls::NB * Cls::ND + Cls::NA * Cls::ND + Cls::NB * Cls::NC +
+                                Cls::NA * Cls::NC;
+    static constexpr int PER_WARP = ACC + WORK + DBLK;   // doubles
+};
+
+template <int La, int Lb, int Lc, int Ld>
+__device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, double* acc, double* V, double* Db,
+                                             int lane, int* nq_done, int* np_done) {
+    using Cls = EriClass<La, Lb, Lc, Ld>;
+    using Lay = CoopLayout<La, Lb, Lc, Ld>;
+    constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND, NE = Cls::NE, NF = Cls::NF;
+    constexpr int NAB = Lay::NAB, NCD = Lay::NCD, M = Cls::M;
+    const int n = d.nbasis, ns = d.nshell;
+    const int qa = d.pr_qa[P], qb = d.pr_qb[P], qc = d.pr_qa[Q], qd = d.pr_qb[Q];
+    const int sa = d.q_parent[qa], sb = d.q_parent[qb], sc = d.q_parent[qc], sd = d.q_parent[qd];
+    const double* cm = d.cutmat;
+    double dnmax = fmax(4.0 * cm[sa * ns + sb], 4.0 * cm[sc * ns + sd]);
+    dnmax = fmax(dnmax, fmax(cm[sa * ns + sd], cm[sa * ns + sc]));
+    dnmax = fmax(dnmax, fmax(cm[sb * ns + sc], cm[sb * ns + sd]));
+    const double ct = d.pr_Y[P] * d.pr_Y[Q];
+    if (!(ct * dnmax > d.cut)) return;            // warp-uniform
+    if (lane == 0) ++*nq_done;
+    const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
+    const double ABx = d.xyz[3 * ia] - d.xyz[3 * ib], ABy = d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
+                 ABz = d.xyz[3 * ia + 2] - d.xyz[3 * ib + 2];
+    const double Cx = d.xyz[3 * ic], Cy = d.xyz[3 * ic + 1], Cz = d.xyz[3 * ic + 2];
+    const double CDx = Cx - d.xyz[3 * id], CDy = Cy - d.xyz[3 * id + 1], CDz = Cz - d.xyz[3 * id + 2];
+
+    for (int t = lane; t < Lay::ACC; t += 32) acc[t] = 0.0;
+    if (lane == 0) V[M + 1] = 0.0;
+    const VrrNode* __restrict__ tab = Cls::nodes();
+    const short* __restrict__ loff = Cls::level_off();
+    const short* __restrict__ tgt = Cls::targets();
+    const int bp0 = d.pr_pp0[P], bnp = d.pr_npp[P], bps = d.pr_pps[P];
+    const int kp0 = d.pr_pp0[Q], knp = d.pr_npp[Q], kps = d.pr_pps[Q];
+    for (int i = 0; i < bnp; ++i) {
+        const int pi = bp0 + i * bps;
+        const double zeta = __ldg(d.pp_zeta + pi), oo2z = __ldg(d.pp_oo2z + pi);
+        const double Kab = __ldg(d.pp_K + pi) * kX0;
+        const double cut1 = dnmax * __ldg(d.pp_cut + pi);
+        const double Px = __ldg(d.pp_Px + pi), Py = __ldg(d.pp_Py + pi), Pz = __ldg(d.pp_Pz + pi);
+        const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
+        for (int j = 0; j < knp; ++j) {
+            const int pj = kp0 + j * kps;
+            if (!(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;   // warp-uniform
+            if (lane == 0) ++*np_done;
+            const double eta = __ldg(d.pp_zeta + pj), oo2e = __ldg(d.pp_oo2z + pj);
+            const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
+            const double s = zeta + eta, rs = rsqrt(s), inv_s = rs * rs;
+            const double rho_z = eta * inv_s, rho_e = zeta * inv_s, rho = zeta * rho_z;
+            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+            const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = Kab * __ldg(d.pp_K + pj) * rs;
+            const double oo2ze = 0.5 * inv_s;
+            const double WPx = -rho_z * PQx, WPy = -rho_z * PQy, WPz = -rho_z * PQz;
+            const double QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
+            const double WQx = rho_e * PQx, WQy = rho_e * PQy, WQz = rho_e * PQz;
+            if (lane <= M) V[lane] = boys_one(lane, T, d.boys) * pref;
+            __syncwarp();
+            for (int L = 0; L < Cls::NLEVEL; ++L) {
+                const int k1 = loff[L + 1];
+                for (int k = loff[L] + lane; k < k1; k += 32) {
+                    const VrrNode nd = tab[k];
+                    double val;
+                    if (nd.kind) {
+                        const double qc = nd.axis == 0 ? QCx : (nd.axis == 1 ? QCy : QCz);
+                        const double wq = nd.axis == 0 ? WQx : (nd.axis == 1 ? WQy : WQz);
+                        val = qc * V[nd.a] + wq * V[nd.b] + nd.n2 * oo2e * (V[nd.c] - rho_e * V[nd.d]) +
+                              nd.na * oo2ze * V[nd.g];
+                    } else {
+                        const double pa = nd.axis == 0 ? PAx : (nd.axis == 1 ? PAy : PAz);
+                        const double wp = nd.axis == 0 ? WPx : (nd.axis == 1 ? WPy : WPz);
+                        val = pa * V[nd.a] + wp * V[nd.b] + nd.n2 * oo2z * (V[nd.c] - rho_z * V[nd.d]);
+                    }
+                    V[M + 2 + k] = val;
+                }
+                __syncwarp();
+            }
+            for (int t = lane; t < Lay::ACC; t += 32) acc[t] += V[tgt[t]];
+            __syncwarp();
+        }
+    }
+    __syncwarp();   // acc complete (also when every primitive quartet was screened out)
+    // bra HRR (one ket column per lane), then ket HRR (one bra row per lane)
+    double* t1 = V;
+    double* I = V + NF * NAB;
+    for (int f = lane; f < NF; f += 32) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, ABx, ABy, ABz);
+    __syncwarp();
+    for (int ab = lane; ab < NAB; ab += 32) Cls::hrr_ket(t1 + ab, NAB, I + ab * NCD, CDx, CDy, CDz);
+    // density blocks
+    const int fa = d.q_f0[qa], fb = d.q_f0[qb], fc = d.q_f0[qc], fd = d.q_f0[qd];
+    double* Dab = Db;
+    double* Dcd = Dab + NAB;
+    double* Dbd = Dcd + NCD;
+    double* Dad = Dbd + NB * ND;
+    double* Dbc = Dad + NA * ND;
+    double* Dac = Dbc + NB * NC;
+    for (int t = lane; t < NAB; t += 32) Dab[t] = d.D[(fa + t / NB) * n + fb + t % NB];
+    for (int t = lane; t < NCD; t += 32) Dcd[t] = d.D[(fc + t / ND) * n + fd + t % ND];
+    for (int t = lane; t < NB * ND; t += 32) Dbd[t] = d.D[(fb + t / ND) * n + fd + t % ND];
+    for (int t = lane; t < NA * ND; t += 32) Dad[t] = d.D[(fa + t / ND) * n + fd + t % ND];
+    for (int t = lane; t < NB * NC; t += 32) Dbc[t] = d.D[(fb + t / NC) * n + fc + t % NC];
+    for (int t = lane; t < NA * NC; t += 32) Dac[t] = d.D[(fa + t / NC) * n + fc + t % NC];
+    __syncwarp();
+    for (int t = lane; t < NAB * NCD; t += 32) {
+        const int ab = t / NCD, cd = t % NCD;
+        I[t] *= Cls::cons_a(ab / NB) * Cls::cons_b(ab % NB) * Cls::cons_c(cd / ND) * Cls::cons_d(cd % ND);
+    }
+    __syncwarp();
+    const double deg = (qa != qb ? 2.0 : 1.0) * (qc != qd ? 2.0 : 1.0) * (P != Q ? 2.0 : 1.0);
+    const double wJ = 0.25 * deg, wK = -0.0625 * deg;
+    constexpr int O1 = NAB, O2 = O1 + NCD, O3 = O2 + NA * NC, O4 = O3 + NB * NC, O5 = O4 + NA * ND,
+                  O6 = O5 + NB * ND;
+    unsigned long long* A = d.A;
+    for (int t = lane; t < O6; t += 32) {
+        double sum = 0.0;
+        size_t addr;
+        double w;
+        if (t < O1) {                 // J over the bra: (ab) row . Dcd
+            for (int cd = 0; cd < NCD; ++cd) sum = fma(I[t * NCD + cd], Dcd[cd], sum);
+            addr = (size_t)(fa + t / NB) * n + fb + t % NB; w = wJ;
+        } else if (t < O2) {          // J over the ket
+            const int cd = t - O1;
+            for (int ab = 0; ab < NAB; ++ab) sum = fma(I[ab * NCD + cd], Dab[ab], sum);
+            addr = (size_t)(fc + cd / ND) * n + fd + cd % ND; w = wJ;
+        } else if (t < O3) {          // K_ac = sum_bd I D_bd
+            const int a = (t - O2) / NC, c = (t - O2) % NC;
+            for (int b = 0; b < NB; ++b)
+                for (int e = 0; e < ND; ++e) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dbd[b * ND + e], sum);
+            addr = (size_t)(fa + a) * n + fc + c; w = wK;
+        } else if (t < O4) {          // K_bc = sum_ad I D_ad
+            const int b = (t - O3) / NC, c = (t - O3) % NC;
+            for (int a = 0; a < NA; ++a)
+                for (int e = 0; e < ND; ++e) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dad[a * ND + e], sum);
+            addr = (size_t)(fb + b) * n + fc + c; w = wK;
+        } else if (t < O5) {          // K_ad = sum_bc I D_bc
+            const int a = (t - O4) / ND, e = (t - O4) % ND;
+            for (int b = 0; b < NB; ++b)
+                for (int c = 0; c < NC; ++c) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dbc[b * NC + c], sum);
+            addr = (size_t)(fa + a) * n + fd + e; w = wK;
+        } else {                      // K_bd = sum_ac I D_ac
+            const int b = (t - O5) / ND, e = (t - O5) % ND;
+            for (int a = 0; a < NA; ++a)
+                for (int c = 0; c < NC; ++c) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dac[a * NC + c], sum);
+            addr = (size_t)(fb + b) * n + fd + e; w = wK;
+        }
+        atomic_fixed(A + addr, w * sum);
+    }
+    __syncwarp();
+}
+
+constexpr int kCoopWarps = 4;
+
+template <int La, int Lb, int Lc, int Ld>
+__global__ void __launch_bounds__(32 * kCoopWarps)
+fock_coop_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __restrict__ counter) {
+    using Lay = CoopLayout<La, Lb, Lc, Ld>;
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* acc = smem + (size_t)warp * Lay::PER_WARP;
+    double* V = acc + Lay::ACC;
+    double* Db = V + Lay::WORK;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        int nq = 0, np = 0;
+        for (int k = 0; k < w.z; ++k) coop_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + k, acc, V, Db, lane, &nq, &np);
+        if (d.stats && lane == 0) {
+            atomicAdd(d.stats, (unsigned long long)nq);
+            atomicAdd(d.stats + 1, (unsigned long long)np);
+        }
+    }
+}
+
 // Work item: x = bra pair, y = first ket pair, z = number of kets (<= 32).
 template <int La, int Lb, int Lc, int Ld>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
@@ -312,10 +533,11 @@ schwarz_kernel(DevData d, const int2* __restrict__ work, int n_work, const int* 
                           d.xyz[3 * ia + 2] - d.xyz[3 * ib + 2]};
     const double Cc[3] = {d.xyz[3 * ia], d.xyz[3 * ia + 1], d.xyz[3 * ia + 2]};
     int p0 = d.pr_pp0[P], np = d.pr_npp[P];
-    if (mode >= 0) { p0 += mode; np = 1; }
+    const int ps = d.pr_pps[P];
+    if (mode >= 0) { p0 += mode * ps; np = 1; }
     double acc[NE * NF];
     int ndone = 0;
-    contract_quartet<La, Lb, La, Lb>(d, p0, np, p0, np, Cc, 0.0, false, acc, &ndone);
+    contract_quartet<La, Lb, La, Lb>(d, p0, np, ps, p0, np, ps, Cc, 0.0, false, acc, &ndone);
     double t1[NF * NAB];
 #pragma unroll
     for (int f = 0; f < NF; ++f) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, AB[0], AB[1], AB[2]);
@@ -424,35 +646,57 @@ struct Bucket {
     int La, Lb, npa, npb, begin, end;
 };
 
+// Primitive-pair data is stored bucket-interleaved: primitive pair k of pair P sits
+// at pp0[P] + k * pps[P] with pps = bucket size, so the 32 consecutive ket pairs of
+// a warp item read consecutive addresses (coalesced).
 struct PairTable {
-    std::vector<int> qa, qb, pp0, npp;
+    std::vector<int> qa, qb, pp0, npp, pps;
     std::vector<double> Y;
-    std::vector<double> zeta, oo2z, K, cut, P, PA;
+    std::vector<double> zeta, oo2z, K, cut, Px, Py, Pz, PAx, PAy, PAz;
     std::vector<Bucket> buckets;
-    DevBuf<int> d_qa, d_qb, d_pp0, d_npp;
-    DevBuf<double> d_Y, d_zeta, d_oo2z, d_K, d_cut, d_P, d_PA;
+    DevBuf<int> d_qa, d_qb, d_pp0, d_npp, d_pps;
+    DevBuf<double> d_Y, d_zeta, d_oo2z, d_K, d_cut, d_Px, d_Py, d_Pz, d_PAx, d_PAy, d_PAz;
     void clear() {
-        qa.clear(); qb.clear(); pp0.clear(); npp.clear(); Y.clear();
-        zeta.clear(); oo2z.clear(); K.clear(); cut.clear(); P.clear(); PA.clear(); buckets.clear();
+        qa.clear(); qb.clear(); pp0.clear(); npp.clear(); pps.clear(); Y.clear();
+        zeta.clear(); oo2z.clear(); K.clear(); cut.clear();
+        Px.clear(); Py.clear(); Pz.clear(); PAx.clear(); PAy.clear(); PAz.clear(); buckets.clear();
     }
 };
 
-using FockFn = void (*)(dim3, dim3, cudaStream_t, const DevData&, const int4*, int, int*);
+using FockFn = void (*)(dim3, dim3, size_t, cudaStream_t, const DevData&, const int4*, int, int*);
 template <int a, int b, int c, int e>
-void launch_fock(dim3 g, dim3 bl, cudaStream_t s, const DevData& dd, const int4* it, int n, int* cnt) {
-    fock_class_kernel<a, b, c, e><<<g, bl, 0, s>>>(dd, it, n, cnt);
+void launch_fock(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData& dd, const int4* it, int n, int* cnt) {
+    if constexpr (EriClass<a, b, c, e>::COOP)
+        fock_coop_kernel<a, b, c, e><<<g, bl, smem, s>>>(dd, it, n, cnt);
+    else
+        fock_class_kernel<a, b, c, e><<<g, bl, 0, s>>>(dd, it, n, cnt);
 }
 template <int a, int b, int c, int e>
-const void* fock_fn_ptr() { return (const void*)&fock_class_kernel<a, b, c, e>; }
+const void* fock_fn_ptr() {
+    if constexpr (EriClass<a, b, c, e>::COOP)
+        return (const void*)&fock_coop_kernel<a, b, c, e>;
+    else
+        return (const void*)&fock_class_kernel<a, b, c, e>;
+}
+template <int a, int b, int c, int e>
+constexpr size_t coop_smem() {
+    if constexpr (EriClass<a, b, c, e>::COOP)
+        return sizeof(double) * kCoopWarps * CoopLayout<a, b, c, e>::PER_WARP;
+    else
+        return 0;
+}
 
 struct ClassEntry {
     int La, Lb, Lc, Ld;
     FockFn fn;
     const void* (*kernel)();
     double prim_flops, quartet_flops;   // algorithmic FP64 operations (gen_eri.py model)
+    bool coop;                          // one quartet per warp (high angular momentum)
+    size_t smem;                        // dynamic shared memory of a block (coop only)
 };
 #define QK_X(a, b, c, e) {a, b, c, e, &launch_fock<a, b, c, e>, &fock_fn_ptr<a, b, c, e>, \
-                          EriClass<a, b, c, e>::PRIM_FLOPS, EriClass<a, b, c, e>::QUARTET_FLOPS},
+                          EriClass<a, b, c, e>::PRIM_FLOPS, EriClass<a, b, c, e>::QUARTET_FLOPS, \
+                          EriClass<a, b, c, e>::COOP, coop_smem<a, b, c, e>()},
 static const ClassEntry g_classes[] = {QK_ERI_CLASS_LIST(QK_X)};
 #undef QK_X
 constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
@@ -495,6 +739,11 @@ struct qk_ctx {
     cudaEvent_t ev[2 * qk::kNumClasses] = {};
     bool ev_recorded[qk::kNumClasses] = {};
     qk::DevBuf<unsigned long long> d_stats;
+    // concurrent class launches: fork/join over auxiliary streams
+    static constexpr int kAux = 4;
+    cudaStream_t aux[kAux] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
+    std::vector<int> launch_order;   // class indices, coop classes first, then by listed work
     // drop-in (reference-shaped) state
     std::vector<double> host_D, host_cutmat;
     bool have_D = false, have_cutmat = false;
@@ -562,13 +811,18 @@ static DevData make_devdata(qk_ctx* c) {
     d.pr_qb = c->pairs.d_qb.p;
     d.pr_pp0 = c->pairs.d_pp0.p;
     d.pr_npp = c->pairs.d_npp.p;
+    d.pr_pps = c->pairs.d_pps.p;
     d.pr_Y = c->pairs.d_Y.p;
     d.pp_zeta = c->pairs.d_zeta.p;
     d.pp_oo2z = c->pairs.d_oo2z.p;
     d.pp_K = c->pairs.d_K.p;
     d.pp_cut = c->pairs.d_cut.p;
-    d.pp_P = c->pairs.d_P.p;
-    d.pp_PA = c->pairs.d_PA.p;
+    d.pp_Px = c->pairs.d_Px.p;
+    d.pp_Py = c->pairs.d_Py.p;
+    d.pp_Pz = c->pairs.d_Pz.p;
+    d.pp_PAx = c->pairs.d_PAx.p;
+    d.pp_PAy = c->pairs.d_PAy.p;
+    d.pp_PAz = c->pairs.d_PAz.p;
     d.boys = c->d_boys.p;
     d.cut = c->integralCutoff;
     d.primLimit = c->primLimit;
@@ -618,27 +872,50 @@ static void build_pairs(qk_ctx* c, bool screened) {
         T.qa.push_back(cand[k].qa);
         T.qb.push_back(cand[k].qb);
         T.Y.push_back(cand[k].Y);
-        T.pp0.push_back((int)T.zeta.size());
         T.npp.push_back(a.nprim * b.nprim);
+    }
+    // primitive-pair placement: bucket-interleaved (screened) or pair-major (one
+    // bucket per pair when unscreened)
+    const int np = (int)cand.size();
+    T.pp0.assign(np, 0);
+    T.pps.assign(np, 1);
+    size_t total = 0;
+    if (screened) {
+        for (const Bucket& B : T.buckets) {
+            const int m = B.end - B.begin;
+            for (int P = B.begin; P < B.end; ++P) {
+                T.pp0[P] = (int)(total + (P - B.begin));
+                T.pps[P] = m;
+            }
+            total += (size_t)m * B.npa * B.npb;
+        }
+    } else {
+        for (int P = 0; P < np; ++P) {
+            T.pp0[P] = (int)total;
+            total += T.npp[P];
+        }
+    }
+    T.zeta.assign(total, 0.0); T.oo2z.assign(total, 0.0); T.K.assign(total, 0.0); T.cut.assign(total, 0.0);
+    T.Px.assign(total, 0.0); T.Py.assign(total, 0.0); T.Pz.assign(total, 0.0);
+    T.PAx.assign(total, 0.0); T.PAy.assign(total, 0.0); T.PAz.assign(total, 0.0);
+    for (int P = 0; P < np; ++P) {
+        const Qsh &a = c->qsh[T.qa[P]], &b = c->qsh[T.qb[P]];
         const double* A = &c->xyz[3 * a.atom];
         const double* B = &c->xyz[3 * b.atom];
         const double r2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
         for (int i = 0; i < a.nprim; ++i)
             for (int j = 0; j < b.nprim; ++j) {
+                const size_t at = (size_t)T.pp0[P] + (size_t)(i * b.nprim + j) * T.pps[P];
                 const double ea = a.expo[i], eb = b.expo[j], z = ea + eb;
                 // Xcoeff without X0 (src/modules/include/eri.fh:118-140)
-                const double Kab = std::exp(-ea * eb / z * r2) / z * a.coef[i] * b.coef[j];
-                double cp = 0.0;
-                if (screened) cp = c->cutprim[(size_t)(a.prim0 + i) * c->jbasis + (b.prim0 + j)];
-                T.zeta.push_back(z);
-                T.oo2z.push_back(0.5 / z);
-                T.K.push_back(Kab);
-                T.cut.push_back(cp);
-                for (int x = 0; x < 3; ++x) {
-                    const double Px = (A[x] * ea + B[x] * eb) / z;
-                    T.P.push_back(Px);
-                    T.PA.push_back(Px - A[x]);
-                }
+                T.K[at] = std::exp(-ea * eb / z * r2) / z * a.coef[i] * b.coef[j];
+                T.cut[at] = screened ? c->cutprim[(size_t)(a.prim0 + i) * c->jbasis + (b.prim0 + j)] : 0.0;
+                T.zeta[at] = z;
+                T.oo2z[at] = 0.5 / z;
+                const double px = (A[0] * ea + B[0] * eb) / z, py = (A[1] * ea + B[1] * eb) / z,
+                             pz = (A[2] * ea + B[2] * eb) / z;
+                T.Px[at] = px; T.Py[at] = py; T.Pz[at] = pz;
+                T.PAx[at] = px - A[0]; T.PAy[at] = py - A[1]; T.PAz[at] = pz - A[2];
             }
     }
 }
@@ -650,13 +927,18 @@ static int upload_pairs(qk_ctx* c) {
     QK_CUDA_TRY(T.d_qb.upload(T.qb, s));
     QK_CUDA_TRY(T.d_pp0.upload(T.pp0, s));
     QK_CUDA_TRY(T.d_npp.upload(T.npp, s));
+    QK_CUDA_TRY(T.d_pps.upload(T.pps, s));
     QK_CUDA_TRY(T.d_Y.upload(T.Y, s));
     QK_CUDA_TRY(T.d_zeta.upload(T.zeta, s));
     QK_CUDA_TRY(T.d_oo2z.upload(T.oo2z, s));
     QK_CUDA_TRY(T.d_K.upload(T.K, s));
     QK_CUDA_TRY(T.d_cut.upload(T.cut, s));
-    QK_CUDA_TRY(T.d_P.upload(T.P, s));
-    QK_CUDA_TRY(T.d_PA.upload(T.PA, s));
+    QK_CUDA_TRY(T.d_Px.upload(T.Px, s));
+    QK_CUDA_TRY(T.d_Py.upload(T.Py, s));
+    QK_CUDA_TRY(T.d_Pz.upload(T.Pz, s));
+    QK_CUDA_TRY(T.d_PAx.upload(T.PAx, s));
+    QK_CUDA_TRY(T.d_PAy.upload(T.PAy, s));
+    QK_CUDA_TRY(T.d_PAz.upload(T.PAz, s));
     return QK_OK;
 }
 
@@ -705,15 +987,34 @@ static int build_work(qk_ctx* c) {
         for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
         QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
         if (!W.items.empty()) {
+            const int wpb = ce.coop ? kCoopWarps : kWarpsPerBlock;
+            if (ce.smem > 48 * 1024)
+                QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
             int bps = 0;
-            QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(), 32 * kWarpsPerBlock, 0));
-            bps = std::max(bps, 1);
-            const long long need = ((long long)W.items.size() + kWarpsPerBlock - 1) / kWarpsPerBlock;
+            QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(), 32 * wpb, ce.smem));
+            if (bps < 1) return fail(QK_ERR_CUDA, "class kernel cannot be resident");
+            const long long need = ((long long)W.items.size() + wpb - 1) / wpb;
             W.grid = (int)std::min<long long>((long long)bps * c->num_sms, need);
             c->launches++;
         }
     }
     c->launches += 1;  // finalize
+    c->launch_order.clear();
+    for (int ci = 0; ci < kNumClasses; ++ci)
+        if (!c->work[ci].items.empty()) c->launch_order.push_back(ci);
+    std::stable_sort(c->launch_order.begin(), c->launch_order.end(), [&](int x, int y) {
+        if (g_classes[x].coop != g_classes[y].coop) return g_classes[x].coop;
+        const double wx = c->work[x].nprimq * g_classes[x].prim_flops + c->work[x].nquart * g_classes[x].quartet_flops;
+        const double wy = c->work[y].nprimq * g_classes[y].prim_flops + c->work[y].nquart * g_classes[y].quartet_flops;
+        return wx > wy;
+    });
+    if (!c->fork_ev) {
+        QK_CUDA_TRY(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+        for (int k = 0; k < qk_ctx::kAux; ++k) {
+            QK_CUDA_TRY(cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+            QK_CUDA_TRY(cudaEventCreateWithFlags(&c->join_ev[k], cudaEventDisableTiming));
+        }
+    }
     return QK_OK;
 }
 
@@ -758,22 +1059,45 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         QK_CUDA_TRY(cudaMemsetAsync(c->d_stats.p, 0, sizeof(unsigned long long) * 2 * kNumClasses, s));
     }
     long long nq = 0, npq = 0;
-    for (int ci = 0; ci < kNumClasses; ++ci) {
+    for (int ci = 0; ci < kNumClasses; ++ci) c->ev_recorded[ci] = false;
+    // Classes run concurrently on auxiliary streams forked from `s` (the high
+    // angular momentum, latency-bound classes first so the bulk classes fill the
+    // remaining SMs).  With per-class event timing on they run one after another
+    // on `s`, so that every class kernel is timed alone.
+    const bool concurrent = !c->profile_events;
+    if (concurrent) QK_CUDA_TRY(cudaEventRecord(c->fork_ev, s));
+    bool used[qk_ctx::kAux] = {};
+    int slot = 0;
+    for (int ci : c->launch_order) {
         ClassWork& W = c->work[ci];
-        c->ev_recorded[ci] = false;
-        if (W.items.empty()) continue;
+        cudaStream_t ls = s;
+        if (concurrent) {
+            const int k = slot++ % qk_ctx::kAux;
+            ls = c->aux[k];
+            if (!used[k]) {
+                QK_CUDA_TRY(cudaStreamWaitEvent(ls, c->fork_ev, 0));
+                used[k] = true;
+            }
+        }
         if (c->profile_stats) d.stats = c->d_stats.p + 2 * ci;
-        if (c->profile_events) QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci], s));
-        g_classes[ci].fn(dim3(W.grid), dim3(32 * kWarpsPerBlock), s, d, W.d_items.p, (int)W.items.size(),
-                         c->d_counters.p + ci);
+        if (c->profile_events) QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci], ls));
+        const ClassEntry& ce = g_classes[ci];
+        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? kCoopWarps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
+              (int)W.items.size(), c->d_counters.p + ci);
         QK_CUDA_TRY(cudaGetLastError());
         if (c->profile_events) {
-            QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci + 1], s));
+            QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci + 1], ls));
             c->ev_recorded[ci] = true;
         }
         nq += W.nquart;
         npq += W.nprimq;
     }
+    if (concurrent)
+        for (int k = 0; k < qk_ctx::kAux; ++k)
+            if (used[k]) {
+                QK_CUDA_TRY(cudaEventRecord(c->join_ev[k], c->aux[k]));
+                QK_CUDA_TRY(cudaStreamWaitEvent(s, c->join_ev[k], 0));
+            }
     finalize_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(c->d_A.p, n, o);
     QK_CUDA_TRY(cudaGetLastError());
     c->last_quart = nq;
@@ -853,6 +1177,11 @@ int qk_destroy(qk_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& a : c->aux)
+        if (a) cudaStreamDestroy(a);
+    for (auto& e : c->join_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     cudaStreamDestroy(c->stream);
     delete c;
     return QK_OK;
