@@ -977,8 +977,12 @@ static int build_work(qk_ctx* c) {
                     if (nk <= 0) continue;
                     W.nquart += nk;
                     W.nprimq += (long long)T.npp[P] * K.npa * K.npb * nk;
-                    for (int s = 0; s < nk; s += 32)
-                        tmp.push_back({make_int4(P, K.begin + s, std::min(32, nk - s), 0), cost});
+                    // per-lane classes: up to 32 kets per warp item; cooperative classes
+                    // (one quartet per warp at a time): one ket per item, so that the
+                    // few, long quartets spread over many warps
+                    const int chunk = ce.coop ? 1 : 32;
+                    for (int s = 0; s < nk; s += chunk)
+                        tmp.push_back({make_int4(P, K.begin + s, std::min(chunk, nk - s), 0), cost});
                 }
             }
         }
@@ -1104,6 +1108,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     c->last_primq = npq;
     return QK_OK;
 }
+
 
 }  // namespace qk
 
