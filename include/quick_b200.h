@@ -132,6 +132,22 @@ int qk_fock2e_host(qk_ctx *ctx, const double *D, const double *cutmat, double *o
  * (stream: a cudaStream_t, NULL = the CUDA default stream). */
 int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_dev, void *stream);
 
+/* Allocation-free Fock build (no counterpart in the reference).  Same arguments and
+ * result as qk_fock2e_device, for callers that must not allocate device memory at the
+ * point of the build -- a program that fixes its memory pool at start-up, or code
+ * that may not call cudaMalloc/cudaFree because they synchronise the device.  The
+ * per-build scratch (the fixed-point accumulator, the work counters and, when
+ * cutmat_dev is NULL, the density screen) lives in one array inside the library that
+ * every GPU loading it holds until exit: limits nbasis <= 1024 and, with
+ * cutmat_dev == NULL, nshell <= 512; larger sizes return QK_ERR_INVALID_ARG.
+ * The pair tables must already exist: run qk_fock2e_device once after any basis,
+ * Schwarz or cutoff change, else QK_ERR_NOT_READY.  The first call on a device looks
+ * up the array's device address; make it before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU race: keep them on one stream (or order
+ * them with events). */
+int qk_fock2e_device_noalloc(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
+                             double *o_dev, void *stream);
+
 /* Work statistics of the last build: shell quartets listed and primitive quartets
  * listed after Schwarz screening (before density screening). */
 int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int *launches);

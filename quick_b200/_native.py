@@ -21,7 +21,7 @@ EXPORTED = [
     "qk_destroy", "qk_default_ctx", "qk_set_basis", "qk_schwarz", "qk_set_schwarz",
     "qk_set_cutoffs", "qk_fock2e_device", "qk_fock2e_host", "qk_density_cutoff_device",
     "qk_last_work", "qk_launches_per_build", "qk_oei_host", "qk_set_profiling",
-    "qk_class_profile", "qk_fp64_peak",
+    "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc",
 ]
 
 _lib = None
@@ -68,6 +68,8 @@ def lib():
     L.qk_class_profile.argtypes = [P, I, P, P, P, P, P, P, P, P]
     L.qk_class_profile.restype = I
     L.qk_fp64_peak.argtypes = [I, ctypes.POINTER(ctypes.c_double)]
+    L.qk_fock2e_device_noalloc.argtypes = [P, P, P, P, P]
+    L.qk_fock2e_device_noalloc.restype = I
     for name in EXPORTED:
         if name.startswith("gpu_"):
             getattr(L, name).restype = None

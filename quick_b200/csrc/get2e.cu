@@ -1110,6 +1110,108 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
 }
 
 
+// ------------------------------------------------------------------ fixed scratch
+// Scratch of the allocation-free build (qk_fock2e_device_noalloc).  Some callers
+// may not allocate device memory at the point where they need a Fock build (a
+// host program whose memory pool is fixed after start-up, a section that must
+// not call cudaMalloc/cudaFree because those synchronise the device, or a
+// runtime that hands this library only the buffers it owns).  For them the
+// per-build scratch -- the int64 accumulator, the work counters and, when the
+// caller passes no density screen, that screen -- lives in this file-scope
+// array, which every GPU that loads the library holds until the process exits.
+// Layout in 8-byte words: [A: kNoAllocMaxNbasis^2][cutmat: kNoAllocMaxNshell^2]
+// [counters: kNumClasses ints].
+constexpr int kNoAllocMaxNbasis = 1024;
+constexpr int kNoAllocMaxNshell = 512;
+constexpr size_t kNoAllocWordsA = (size_t)kNoAllocMaxNbasis * kNoAllocMaxNbasis;
+constexpr size_t kNoAllocWordsCut = (size_t)kNoAllocMaxNshell * kNoAllocMaxNshell;
+constexpr size_t kNoAllocWords = kNoAllocWordsA + kNoAllocWordsCut + (kNumClasses + 1) / 2 + 1;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
+
+// Device address of g_noalloc_scratch, looked up once per device (in host code the
+// symbol's name is only a stand-in for the device array, never a usable pointer).
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+static int noalloc_scratch(int device, unsigned long long** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(QK_ERR_UNSUPPORTED, "device index too large");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        // the caller made `device` current
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "quick_b200: cudaGetSymbolAddress(scratch) failed: %s\n", cudaGetErrorString(e));
+            g_last_status = QK_ERR_CUDA;
+            return QK_ERR_CUDA;
+        }
+        g_noalloc_ptr[device] = (unsigned long long*)p;
+    }
+    *out = g_noalloc_ptr[device];
+    return QK_OK;
+}
+
+// The same build as fock2e_device with its scratch taken from g_noalloc_scratch;
+// it calls no allocator.  The pair tables and work lists must already exist.
+static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s) {
+    if (c->nbasis > kNoAllocMaxNbasis)
+        return fail(QK_ERR_INVALID_ARG, "qk_fock2e_device_noalloc: nbasis exceeds the fixed scratch (max 1024)");
+    if (!cutmat && c->nshell > kNoAllocMaxNshell)
+        return fail(QK_ERR_INVALID_ARG,
+                    "qk_fock2e_device_noalloc: nshell exceeds the fixed density-screen scratch (max 512); "
+                    "pass cutmat_dev");
+    if (!c->have_basis || !c->have_schwarz || c->pairs_dirty || c->built_cut != c->integralCutoff)
+        return fail(QK_ERR_NOT_READY,
+                    "qk_fock2e_device_noalloc: pair tables not built for the current basis/Schwarz/cutoffs; "
+                    "run qk_fock2e_device once first");
+    unsigned long long* base = nullptr;
+    int st = noalloc_scratch(c->device, &base);
+    if (st) return st;
+    unsigned long long* A = base;
+    double* cut_scratch = (double*)(base + kNoAllocWordsA);
+    int* counters = (int*)(base + kNoAllocWordsA + kNoAllocWordsCut);
+    const int n = c->nbasis, ns = c->nshell;
+    if (!cutmat) {
+        density_cutoff_kernel<<<(ns * ns + 127) / 128, 128, 0, s>>>(D, n, ns, c->d_shell_f0.p,
+                                                                     c->d_shell_f1.p, cut_scratch);
+        QK_CUDA_TRY(cudaGetLastError());
+        cutmat = cut_scratch;
+    }
+    // the array keeps the previous call's contents: clear what must start at zero
+    QK_CUDA_TRY(cudaMemsetAsync(A, 0, sizeof(unsigned long long) * n * n, s));
+    QK_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * kNumClasses, s));
+    DevData d = make_devdata(c);
+    d.D = D;
+    d.cutmat = cutmat;
+    d.A = A;
+    d.stats = nullptr;
+    QK_CUDA_TRY(cudaEventRecord(c->fork_ev, s));
+    bool used[qk_ctx::kAux] = {};
+    int slot = 0;
+    for (int ci : c->launch_order) {
+        const ClassWork& W = c->work[ci];
+        const int k = slot++ % qk_ctx::kAux;
+        cudaStream_t ls = c->aux[k];
+        if (!used[k]) {
+            QK_CUDA_TRY(cudaStreamWaitEvent(ls, c->fork_ev, 0));
+            used[k] = true;
+        }
+        const ClassEntry& ce = g_classes[ci];
+        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? kCoopWarps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
+              (int)W.items.size(), counters + ci);
+        QK_CUDA_TRY(cudaGetLastError());
+    }
+    for (int k = 0; k < qk_ctx::kAux; ++k)
+        if (used[k]) {
+            QK_CUDA_TRY(cudaEventRecord(c->join_ev[k], c->aux[k]));
+            QK_CUDA_TRY(cudaStreamWaitEvent(s, c->join_ev[k], 0));
+        }
+    finalize_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(A, n, o);
+    QK_CUDA_TRY(cudaGetLastError());
+    return QK_OK;
+}
+
 }  // namespace qk
 
 using namespace qk;
@@ -1409,6 +1511,19 @@ int qk_fock2e_host(qk_ctx* c, const double* D, const double* cutmat, double* o) 
     QK_CUDA_TRY(cudaStreamSynchronize(s));
     for (size_t i = 0; i < G.size(); ++i) o[i] += G[i];
     return QK_OK;
+}
+
+// Allocation-free variant of qk_fock2e_device for callers that may not allocate
+// device memory when they run a Fock build; see the comment at g_noalloc_scratch.
+// Its first call on a device looks up the scratch array's device address (one
+// cudaGetSymbolAddress); make that first call before any stream capture.  All
+// calls share the one scratch array, so calls that overlap on the GPU race:
+// serialise them (one stream, or events between streams).
+int qk_fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutmat, double* o, void* stream) {
+    if (!c || !D || !o) return fail(QK_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    return fock2e_device_noalloc(c, D, cutmat, o, (cudaStream_t)stream);
 }
 
 int qk_last_work(qk_ctx* c, long long* quartets, long long* primq, int* launches) {

@@ -1,0 +1,72 @@
+"""GPU test of the allocation-free Fock build, qk_fock2e_device_noalloc.
+
+Some callers of this library cannot allocate device memory when they need a
+Fock build: a host program that fixes its GPU memory pool at start-up, or code
+that must not call cudaMalloc/cudaFree because those synchronise the whole
+device.  The allocation-free entry point serves them: its per-build scratch
+lives in a fixed array inside the library, and the caller passes only the
+density and the output buffer.
+
+The test drives that entry point through the C ABI and checks its result
+against the ordinary entry point (qk_fock2e_device) on the same density, within
+the Fock tolerance of the other GPU tests, on two calls in a row (the second
+call reuses the scratch that the first one left behind).  This file is named so
+that pytest collects it last; it also passes when run alone in a fresh process.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+FOCK_TOL = 1e-9
+
+
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _random_density(n, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(n, n)) * 0.15
+    return X @ X.T / n ** 0.5
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    _cuda()
+    from quick_b200 import _native
+    from quick_b200.basis import build_basis
+    from quick_b200.get2e import Get2e
+    from quick_b200.molecules import water_cluster
+
+    L = _native.lib()
+    b = build_basis(water_cluster(3, 6.0, seed=11), "6-31G*")
+    eng = Get2e(b, integral_cutoff=1e-10, prim_limit=1e-11)
+    h = ctypes.c_void_p(eng.h)
+    n = b.nbasis
+    stream = torch.cuda.current_stream()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    D = torch.tensor(_random_density(n, 21), device="cuda")
+    # before any ordinary build the pair tables do not exist yet: a clear refusal
+    o = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    assert L.qk_fock2e_device_noalloc(h, vp(D), None, vp(o), ctypes.c_void_p(stream.cuda_stream)) == 102
+
+    ref = eng.fock2e(D).cpu().numpy()          # ordinary entry point (builds the tables)
+    for call in range(2):
+        o = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        st = L.qk_fock2e_device_noalloc(h, vp(D), None, vp(o), ctypes.c_void_p(stream.cuda_stream))
+        assert st == 0, (call, st)
+        got = o.cpu().numpy()
+        err = float(np.abs(got - ref).max())
+        assert err <= FOCK_TOL, (call, err)
+
+    # a caller-provided density screen goes through the same path
+    cm = eng.density_cutoff(D)
+    o = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    assert L.qk_fock2e_device_noalloc(h, vp(D), vp(cm), vp(o), ctypes.c_void_p(stream.cuda_stream)) == 0
+    assert float(np.abs(o.cpu().numpy() - ref).max()) <= FOCK_TOL
+    eng.close()
