@@ -48,6 +48,9 @@ def workload(name):
     elif name == "c40h82-631gss":
         mol, bas = M.c40h82_631gss()
         desc = "C40H82 all-trans (seed 20261203), RHF/6-31G** (6d)"
+    elif name == "w12-ccpvtz":
+        mol, bas = M.water12_ccpvtz()
+        desc = "12 H2O (seed 20261203, 8 A cube), RHF/cc-pVTZ (Cartesian, f on O)"
     else:
         raise SystemExit(f"unknown workload {name}")
     return build_basis(mol, bas), desc

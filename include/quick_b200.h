@@ -92,7 +92,7 @@ int qk_last_status(void);
 const char *qk_status_string(int status);
 /* Rows of gccoeff/gcexpo expected by gpu_upload_basis_ (reference MAXPRIM; default 20). */
 int qk_set_maxprim(int maxprim);
-/* Largest angular momentum per shell compiled into the kernels (2 = d). */
+/* Largest angular momentum per shell compiled into the kernels (3 = f). */
 int qk_max_l(void);
 
 /* Create / destroy a context on CUDA device `device`. */
@@ -174,7 +174,7 @@ int qk_fp64_peak(int device, double *gflops);
  * layout: ncontract(nbasis), itype(3,nbasis), aexp/dcoeff(maxcontract,nbasis),
  * ncenter(nbasis) 1-based.  Charges: nuclei Z(natom) at xyz(3,natom) plus `next`
  * external point charges ext_q at ext_xyz(3,next) (QM/MM).  Writes S, T, V
- * (nbasis^2, symmetric) to host arrays; functions up to d. */
+ * (nbasis^2, symmetric) to host arrays; functions up to f. */
 int qk_oei_host(int device, int natom, const double *xyz, const double *Z, int nbasis,
                 int maxcontract, const int *ncontract, const int *itype, const double *aexp,
                 const double *dcoeff, const int *ncenter, int next, const double *ext_xyz,

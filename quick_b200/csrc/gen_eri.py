@@ -209,6 +209,18 @@ def best_hrr(La, Lb):
 
 
 COOP_MIN = 150   # NE*NF at or above which a class uses the warp-cooperative kernel
+SMEM_MAX = 227 * 1024   # shared memory of one block
+
+
+def is_coop(La, Lb, Lc, Ld):
+    """Warp-cooperative (one quartet per warp) or per-lane straight-line kernel."""
+    Lab, Lcd = La + Lb, Lc + Ld
+    NE = sum(ncart(L) for L in range(La, Lab + 1))
+    NF = sum(ncart(L) for L in range(Lc, Lcd + 1))
+    nint = ncart(La) * ncart(Lb) * ncart(Lc) * ncart(Ld)
+    if max(La, Lb, Lc, Ld) >= 3:
+        return NE * NF >= 60 or nint > 60
+    return NE * NF >= COOP_MIN
 
 
 def vrr_table(g, targets, M):
@@ -269,7 +281,12 @@ def emit_class(La, Lb, Lc, Ld):
     o.append(f"  static constexpr int VRR_NODES = {g.counter}, HRR_BRA = {len(hb_lines)}, HRR_KET = {len(hk_lines)};")
     pf, qf = class_flops(La, Lb, Lc, Ld)
     o.append(f"  static constexpr double PRIM_FLOPS = {pf}.0, QUARTET_FLOPS = {qf}.0;")
-    # VRR: accumulate acc[f*NE+e] += [e0|f0]^(0) with base F_m already scaled.
+    coop = is_coop(La, Lb, Lc, Ld)
+    # VRR: accumulate acc[f*NE+e] += [e0|f0]^(0) with base F_m already scaled
+    # (per-lane classes only; cooperative classes evaluate the node table instead)
+    vrr_lines = []
+    o_main = o
+    o = vrr_lines
     o.append("  template <typename R>")
     o.append("  static __device__ __forceinline__ void vrr(const R* __restrict__ Fm, const VrrGeom<R>& G, R* __restrict__ acc) {")
     o.append("    const R PAx = G.PA[0], PAy = G.PA[1], PAz = G.PA[2];")
@@ -287,6 +304,9 @@ def emit_class(La, Lb, Lc, Ld):
     for idx, nm in targets:
         o.append(f"    acc[{idx}] += {nm};")
     o.append("  }")
+    o = o_main
+    if not coop:
+        o.extend(vrr_lines)
     # bra HRR on one column: SRC(k) = src[k], out[a*NB+b]
     o.append("  static __device__ __forceinline__ void hrr_bra(const double* __restrict__ src, double* __restrict__ out, double ABx, double ABy, double ABz) {")
     o.append("    (void)ABx; (void)ABy; (void)ABz;")
@@ -316,7 +336,6 @@ def emit_class(La, Lb, Lc, Ld):
     o.append(f"  static __device__ __forceinline__ double cons_b(int i) {{ const double t[{nb}] = {{{cb}}}; return t[i]; }}")
     o.append(f"  static __device__ __forceinline__ double cons_c(int i) {{ const double t[{nc}] = {{{cc}}}; return t[i]; }}")
     o.append(f"  static __device__ __forceinline__ double cons_d(int i) {{ const double t[{nd}] = {{{cd}}}; return t[i]; }}")
-    coop = NE * NF >= COOP_MIN
     o.append(f"  static constexpr bool COOP = {'true' if coop else 'false'};")
     if coop:
         rows, off, tslots = vrr_table(g, targets, M)
@@ -379,7 +398,9 @@ def main(out_dir, lmax=LMAX):
         txt, st = emit_class(*cls)
         parts.append(txt)
         stats.append(st)
-    # class list for the host
+    # pair classes (for the Schwarz kernels) and the class list for the host
+    pcls = [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
+    parts.append("#define QK_PAIR_CLASS_LIST(X) " + " ".join(f"X({a}, {b})" for a, b in pcls))
     parts.append("#define QK_ERI_CLASS_LIST(X) \\")
     lines = [f"  X({a}, {b}, {c}, {d})" for (a, b, c, d) in class_list(lmax)]
     parts.append(" \\\n".join(lines))

@@ -300,38 +300,26 @@ struct CoopLayout {
     static constexpr int DBLK = NAB + NCD + Cls::NB * Cls::ND + Cls::NA * Cls::ND + Cls::NB * Cls::NC +
                                 Cls::NA * Cls::NC;
     static constexpr int PER_WARP = ACC + WORK + DBLK;   // doubles
+    // warps per block: as many as fit 227 KB of shared memory, at most 4
+    static constexpr int FIT = (227 * 1024) / (8 * PER_WARP);
+    static constexpr int WARPS = FIT < 1 ? 1 : (FIT > 4 ? 4 : FIT);
+    static_assert(8 * PER_WARP <= 227 * 1024, "cooperative class does not fit in shared memory");
 };
 
+// Contracted [e0|f0] of one quartet into acc (shared, per warp), the VRR done
+// level by level over the 32 lanes with its values in V (shared, per warp).
 template <int La, int Lb, int Lc, int Ld>
-__device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, double* acc, double* V, double* Db,
-                                             int lane, int* nq_done, int* np_done) {
+__device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp, int bps, int kp0, int knp, int kps,
+                                              double Cx, double Cy, double Cz, double dnmax, bool screen,
+                                              double* acc, double* V, int lane, int* np_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     using Lay = CoopLayout<La, Lb, Lc, Ld>;
-    constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND, NE = Cls::NE, NF = Cls::NF;
-    constexpr int NAB = Lay::NAB, NCD = Lay::NCD, M = Cls::M;
-    const int n = d.nbasis, ns = d.nshell;
-    const int qa = d.pr_qa[P], qb = d.pr_qb[P], qc = d.pr_qa[Q], qd = d.pr_qb[Q];
-    const int sa = d.q_parent[qa], sb = d.q_parent[qb], sc = d.q_parent[qc], sd = d.q_parent[qd];
-    const double* cm = d.cutmat;
-    double dnmax = fmax(4.0 * cm[sa * ns + sb], 4.0 * cm[sc * ns + sd]);
-    dnmax = fmax(dnmax, fmax(cm[sa * ns + sd], cm[sa * ns + sc]));
-    dnmax = fmax(dnmax, fmax(cm[sb * ns + sc], cm[sb * ns + sd]));
-    const double ct = d.pr_Y[P] * d.pr_Y[Q];
-    if (!(ct * dnmax > d.cut)) return;            // warp-uniform
-    if (lane == 0) ++*nq_done;
-    const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
-    const double ABx = d.xyz[3 * ia] - d.xyz[3 * ib], ABy = d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
-                 ABz = d.xyz[3 * ia + 2] - d.xyz[3 * ib + 2];
-    const double Cx = d.xyz[3 * ic], Cy = d.xyz[3 * ic + 1], Cz = d.xyz[3 * ic + 2];
-    const double CDx = Cx - d.xyz[3 * id], CDy = Cy - d.xyz[3 * id + 1], CDz = Cz - d.xyz[3 * id + 2];
-
+    constexpr int M = Cls::M;
     for (int t = lane; t < Lay::ACC; t += 32) acc[t] = 0.0;
     if (lane == 0) V[M + 1] = 0.0;
     const VrrNode* __restrict__ tab = Cls::nodes();
     const short* __restrict__ loff = Cls::level_off();
     const short* __restrict__ tgt = Cls::targets();
-    const int bp0 = d.pr_pp0[P], bnp = d.pr_npp[P], bps = d.pr_pps[P];
-    const int kp0 = d.pr_pp0[Q], knp = d.pr_npp[Q], kps = d.pr_pps[Q];
     for (int i = 0; i < bnp; ++i) {
         const int pi = bp0 + i * bps;
         const double zeta = __ldg(d.pp_zeta + pi), oo2z = __ldg(d.pp_oo2z + pi);
@@ -341,7 +329,7 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
         const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
         for (int j = 0; j < knp; ++j) {
             const int pj = kp0 + j * kps;
-            if (!(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;   // warp-uniform
+            if (screen && !(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;   // warp-uniform
             if (lane == 0) ++*np_done;
             const double eta = __ldg(d.pp_zeta + pj), oo2e = __ldg(d.pp_oo2z + pj);
             const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
@@ -379,6 +367,33 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
             __syncwarp();
         }
     }
+}
+
+template <int La, int Lb, int Lc, int Ld>
+__device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, double* acc, double* V, double* Db,
+                                             int lane, int* nq_done, int* np_done) {
+    using Cls = EriClass<La, Lb, Lc, Ld>;
+    using Lay = CoopLayout<La, Lb, Lc, Ld>;
+    constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND, NE = Cls::NE, NF = Cls::NF;
+    constexpr int NAB = Lay::NAB, NCD = Lay::NCD, M = Cls::M;
+    const int n = d.nbasis, ns = d.nshell;
+    const int qa = d.pr_qa[P], qb = d.pr_qb[P], qc = d.pr_qa[Q], qd = d.pr_qb[Q];
+    const int sa = d.q_parent[qa], sb = d.q_parent[qb], sc = d.q_parent[qc], sd = d.q_parent[qd];
+    const double* cm = d.cutmat;
+    double dnmax = fmax(4.0 * cm[sa * ns + sb], 4.0 * cm[sc * ns + sd]);
+    dnmax = fmax(dnmax, fmax(cm[sa * ns + sd], cm[sa * ns + sc]));
+    dnmax = fmax(dnmax, fmax(cm[sb * ns + sc], cm[sb * ns + sd]));
+    const double ct = d.pr_Y[P] * d.pr_Y[Q];
+    if (!(ct * dnmax > d.cut)) return;            // warp-uniform
+    if (lane == 0) ++*nq_done;
+    const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
+    const double ABx = d.xyz[3 * ia] - d.xyz[3 * ib], ABy = d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
+                 ABz = d.xyz[3 * ia + 2] - d.xyz[3 * ib + 2];
+    const double Cx = d.xyz[3 * ic], Cy = d.xyz[3 * ic + 1], Cz = d.xyz[3 * ic + 2];
+    const double CDx = Cx - d.xyz[3 * id], CDy = Cy - d.xyz[3 * id + 1], CDz = Cz - d.xyz[3 * id + 2];
+
+    coop_contract<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q], d.pr_pps[Q],
+                                  Cx, Cy, Cz, dnmax, true, acc, V, lane, np_done);
     __syncwarp();   // acc complete (also when every primitive quartet was screened out)
     // bra HRR (one ket column per lane), then ket HRR (one bra row per lane)
     double* t1 = V;
@@ -448,7 +463,7 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     __syncwarp();
 }
 
-constexpr int kCoopWarps = 4;
+constexpr int kCoopWarps = 4;   // largest warps-per-block of a cooperative class
 
 template <int La, int Lb, int Lc, int Ld>
 __global__ void __launch_bounds__(32 * kCoopWarps)
@@ -569,6 +584,88 @@ schwarz_kernel(DevData d, const int2* __restrict__ work, int n_work, const int* 
     }
 }
 
+// Schwarz bounds for the cooperative classes: one warp per (pair, mode), the
+// contraction of coop_contract without screening, HRR as in coop_quartet, and
+// the largest diagonal integral |(ab|ab)| of the pair block.
+template <int La, int Lb>
+__global__ void __launch_bounds__(32 * kCoopWarps)
+schwarz_coop_kernel(DevData d, const int2* __restrict__ work, int n_work, const int* __restrict__ q_prim0,
+                    const int* __restrict__ q_nprim, int nshell, int jbasis, unsigned long long* __restrict__ Ysq,
+                    unsigned long long* __restrict__ cpsq) {
+    using Cls = EriClass<La, Lb, La, Lb>;
+    using Lay = CoopLayout<La, Lb, La, Lb>;
+    constexpr int NB = Cls::NB, NE = Cls::NE, NF = Cls::NF, NAB = Lay::NAB, NCD = Lay::NCD;
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    double* acc = smem + (size_t)warp * Lay::PER_WARP;
+    double* V = acc + Lay::ACC;
+    for (int t = blockIdx.x * wpb + warp; t < n_work; t += gridDim.x * wpb) {
+        const int P = work[t].x, mode = work[t].y;
+        const int qa = d.pr_qa[P], qb = d.pr_qb[P];
+        const int ia = d.q_atom[qa], ib = d.q_atom[qb];
+        const double ABx = d.xyz[3 * ia] - d.xyz[3 * ib], ABy = d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
+                     ABz = d.xyz[3 * ia + 2] - d.xyz[3 * ib + 2];
+        int p0 = d.pr_pp0[P], np = d.pr_npp[P];
+        const int ps = d.pr_pps[P];
+        if (mode >= 0) { p0 += mode * ps; np = 1; }
+        int ndone = 0;
+        coop_contract<La, Lb, La, Lb>(d, p0, np, ps, p0, np, ps, d.xyz[3 * ia], d.xyz[3 * ia + 1],
+                                      d.xyz[3 * ia + 2], 0.0, false, acc, V, lane, &ndone);
+        __syncwarp();
+        double* t1 = V;
+        double* I = V + NF * NAB;
+        for (int f = lane; f < NF; f += 32) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, ABx, ABy, ABz);
+        __syncwarp();
+        double ymax = 0.0;
+        for (int ab = lane; ab < NAB; ab += 32) {
+            Cls::hrr_ket(t1 + ab, NAB, I + ab * NCD, ABx, ABy, ABz);
+            const double c = Cls::cons_a(ab / NB) * Cls::cons_b(ab % NB);
+            ymax = fmax(ymax, fabs(I[ab * NCD + ab] * c * c));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ymax = fmax(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+        if (lane == 0) {
+            if (mode < 0) {
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(ymax);
+                const int sa = d.q_parent[qa], sb = d.q_parent[qb];
+                atomicMax(Ysq + (size_t)sa * nshell + sb, bits);
+                atomicMax(Ysq + (size_t)sb * nshell + sa, bits);
+            } else {
+                // QUICK's cutprim: cutprim^2 = X0 * (ij|ij)_prim (see schwarz_kernel)
+                const unsigned long long pbits = (unsigned long long)__double_as_longlong(ymax * kX0);
+                const int nbp = q_nprim[qb];
+                const int gi = q_prim0[qa] + mode / nbp, gj = q_prim0[qb] + mode % nbp;
+                atomicMax(cpsq + (size_t)gi * jbasis + gj, pbits);
+                atomicMax(cpsq + (size_t)gj * jbasis + gi, pbits);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Launch the Schwarz kernel of pair class (a, b): per-thread for the small
+// classes, warp-cooperative for the large ones.
+template <int a, int b>
+static cudaError_t launch_schwarz(const DevData& d, const int2* wl, int n, const int* q_prim0, const int* q_nprim,
+                                  int ns, int jb, unsigned long long* Ysq, unsigned long long* cpsq, int num_sms,
+                                  cudaStream_t s) {
+    if constexpr (EriClass<a, b, a, b>::COOP) {
+        using Lay = CoopLayout<a, b, a, b>;
+        const size_t smem = sizeof(double) * Lay::WARPS * Lay::PER_WARP;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute((const void*)&schwarz_coop_kernel<a, b>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        const int grid = std::min((n + Lay::WARPS - 1) / Lay::WARPS, num_sms * 8);
+        schwarz_coop_kernel<a, b><<<grid, 32 * Lay::WARPS, smem, s>>>(d, wl, n, q_prim0, q_nprim, ns, jb, Ysq, cpsq);
+    } else {
+        schwarz_kernel<a, b><<<(n + 127) / 128, 128, 0, s>>>(d, wl, n, q_prim0, q_nprim, ns, jb, Ysq, cpsq);
+    }
+    return cudaGetLastError();
+}
+
 __global__ void density_cutoff_kernel(const double* __restrict__ D, int n, int nshell,
                                       const int* __restrict__ s_f0, const int* __restrict__ s_f1,
                                       double* __restrict__ cutmat) {
@@ -609,7 +706,6 @@ __global__ void finalize_kernel(const unsigned long long* __restrict__ A, int n,
 // =========================================================================== host
 namespace qk {
 
-#define QK_PAIR_CLASSES(X) X(0, 0) X(1, 0) X(1, 1) X(2, 0) X(2, 1) X(2, 2)
 
 template <typename T>
 struct DevBuf {
@@ -681,7 +777,7 @@ const void* fock_fn_ptr() {
 template <int a, int b, int c, int e>
 constexpr size_t coop_smem() {
     if constexpr (EriClass<a, b, c, e>::COOP)
-        return sizeof(double) * kCoopWarps * CoopLayout<a, b, c, e>::PER_WARP;
+        return sizeof(double) * CoopLayout<a, b, c, e>::WARPS * CoopLayout<a, b, c, e>::PER_WARP;
     else
         return 0;
 }
@@ -693,10 +789,18 @@ struct ClassEntry {
     double prim_flops, quartet_flops;   // algorithmic FP64 operations (gen_eri.py model)
     bool coop;                          // one quartet per warp (high angular momentum)
     size_t smem;                        // dynamic shared memory of a block (coop only)
+    int coop_warps;                     // warps per block of the cooperative kernel
 };
+template <int a, int b, int c, int e>
+constexpr int coop_warps() {
+    if constexpr (EriClass<a, b, c, e>::COOP)
+        return CoopLayout<a, b, c, e>::WARPS;
+    else
+        return 0;
+}
 #define QK_X(a, b, c, e) {a, b, c, e, &launch_fock<a, b, c, e>, &fock_fn_ptr<a, b, c, e>, \
                           EriClass<a, b, c, e>::PRIM_FLOPS, EriClass<a, b, c, e>::QUARTET_FLOPS, \
-                          EriClass<a, b, c, e>::COOP, coop_smem<a, b, c, e>()},
+                          EriClass<a, b, c, e>::COOP, coop_smem<a, b, c, e>(), coop_warps<a, b, c, e>()},
 static const ClassEntry g_classes[] = {QK_ERI_CLASS_LIST(QK_X)};
 #undef QK_X
 constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
@@ -991,7 +1095,7 @@ static int build_work(qk_ctx* c) {
         for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
         QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
         if (!W.items.empty()) {
-            const int wpb = ce.coop ? kCoopWarps : kWarpsPerBlock;
+            const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
             if (ce.smem > 48 * 1024)
                 QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
             int bps = 0;
@@ -1086,7 +1190,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         if (c->profile_stats) d.stats = c->d_stats.p + 2 * ci;
         if (c->profile_events) QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci], ls));
         const ClassEntry& ce = g_classes[ci];
-        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? kCoopWarps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
+        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? ce.coop_warps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
               (int)W.items.size(), c->d_counters.p + ci);
         QK_CUDA_TRY(cudaGetLastError());
         if (c->profile_events) {
@@ -1198,7 +1302,7 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
             used[k] = true;
         }
         const ClassEntry& ce = g_classes[ci];
-        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? kCoopWarps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
+        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? ce.coop_warps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
               (int)W.items.size(), counters + ci);
         QK_CUDA_TRY(cudaGetLastError());
     }
@@ -1429,12 +1533,12 @@ int qk_schwarz(qk_ctx* c, double* Yout, double* cpout) {
             if (!v.empty()) {                                                                     \
                 auto& dv = dwl[a * (lmax + 1) + b];                                               \
                 QK_CUDA_TRY(dv.upload(v, c->stream));                                             \
-                schwarz_kernel<a, b><<<((int)v.size() + 127) / 128, 128, 0, c->stream>>>(         \
-                    d, dv.p, (int)v.size(), c->d_q_prim0.p, c->d_q_nprim.p, ns, jb, dY.p, dcp.p); \
-                QK_CUDA_TRY(cudaGetLastError());                                                  \
+                QK_CUDA_TRY((launch_schwarz<a, b>(d, dv.p, (int)v.size(), c->d_q_prim0.p,          \
+                                                  c->d_q_nprim.p, ns, jb, dY.p, dcp.p, c->num_sms, \
+                                                  c->stream)));                                    \
             }                                                                                     \
         }
-        QK_PAIR_CLASSES(QK_SCHWARZ)
+        QK_PAIR_CLASS_LIST(QK_SCHWARZ)
 #undef QK_SCHWARZ
         std::vector<unsigned long long> hY((size_t)ns * ns), hcp((size_t)jb * jb);
         QK_CUDA_TRY(cudaMemcpyAsync(hY.data(), dY.p, hY.size() * 8, cudaMemcpyDeviceToHost, c->stream));

@@ -17,7 +17,7 @@
 
 namespace qk {
 
-constexpr int kOeiLmax = 2;              // per function
+constexpr int kOeiLmax = 3;              // per function (f)
 constexpr int kEj = kOeiLmax + 3;        // j up to l + 2 (kinetic)
 constexpr int kEt = 2 * kOeiLmax + 3;    // t up to i + j
 

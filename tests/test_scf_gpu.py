@@ -20,7 +20,7 @@ def water():
                                                    [0.6735, -0.0019, 0.59353]])
 
 
-@pytest.mark.parametrize("bas", ["STO-3G", "6-31G*", "CC-PVDZ"])
+@pytest.mark.parametrize("bas", ["STO-3G", "6-31G*", "CC-PVDZ", "CC-PVTZ"])
 def test_oei_matches_oracle(bas):
     _cuda()
     from quick_b200.scf import oei
@@ -50,3 +50,21 @@ def test_rhf_matches_oracle_w4_sto3g():
     r = RHF(b, integral_cutoff=1e-10).run(denserms=1e-8)
     assert r["converged"]
     assert abs(r["E"] - ref["E"]) <= 1e-7, (r["E"], ref["E"])
+
+
+def test_rhf_golden_nma_def2tzvp_f_shells():
+    """N-methylacetamide / def2-TZVP (f functions on C, N, O): the reference's CPU
+    golden energy (test/saved/grad_nma_rhf_def2tzvp.out) through the GPU SCF."""
+    _cuda()
+    import json
+    import os
+    from quick_b200.scf import RHF
+    here = os.path.dirname(os.path.abspath(__file__))
+    case = [c for c in json.load(open(os.path.join(here, "golden", "rhf_energies.json")))
+            if c["name"] == "grad_nma_rhf_def2tzvp"][0]
+    m = Molecule.from_angstrom([a[0] for a in case["atoms"]], [a[1:] for a in case["atoms"]], case["charge"])
+    b = build_basis(m, case["basis"])
+    assert b.has_f
+    r = RHF(b, integral_cutoff=1e-11).run(denserms=1e-8)
+    assert r["converged"]
+    assert abs(r["E"] - case["total_energy"]) <= 2e-6, (r["E"], case["total_energy"])
