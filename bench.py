@@ -332,6 +332,32 @@ def run_ours(args):
     G_dev = o.cpu().numpy()
     bit_identical = bool(np.array_equal(G_dev, res))
 
+    # mixed form: FP32 vertical recursion below a Schwarz bound product
+    mixed = None
+    if args.fp32_bound > 0:
+        eng.set_precision(args.fp32_bound)
+        for _ in range(2):
+            o.zero_()
+            eng.fock2e(D, o=o, stream=stream)
+        torch.cuda.synchronize()
+        mixed_ms = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            o.zero_()
+            ev0.record(stream)
+            eng.fock2e(D, o=o, stream=stream)
+            ev1.record(stream)
+            ev1.synchronize()
+            mixed_ms.append(ev0.elapsed_time(ev1))
+        G_mixed = o.cpu().numpy()
+        nq32 = eng.fp32_quartets()
+        eng.set_precision(0.0)
+        mms = float(np.mean(mixed_ms))
+        mixed = {"fp32_bound": args.fp32_bound, "builds_per_s": world * 1000.0 / mms, "ms_per_step": mms,
+                 "speedup_vs_fp64": ms_per_step / mms,
+                 "max_abs_dF_vs_fp64": float(np.abs(G_mixed - G_dev).max()),
+                 "fp32_quartet_fraction": nq32 / max(1, int(ql[:nc].sum()))}
+
     scf = None
     if not args.no_scf:
         rhf = RHF(basis, device=local, engine=eng)
@@ -340,6 +366,14 @@ def run_ours(args):
         scf = {"solves_per_s": round(1.0 / r2["seconds"], 4), "seconds": round(r2["seconds"], 3),
                "iterations": r2["niter"], "E": r2["E"], "converged": bool(r2["converged"]),
                "denserms": 1e-7, "incremental_builds": True}
+        if mixed is not None:
+            eng.set_precision(args.fp32_bound)
+            rhf.run(denserms=1e-7)
+            r3 = rhf.run(denserms=1e-7)
+            eng.set_precision(0.0)
+            mixed["scf"] = {"solves_per_s": round(1.0 / r3["seconds"], 4), "iterations": r3["niter"],
+                            "E": r3["E"], "abs_dE_vs_fp64": abs(r3["E"] - r2["E"]),
+                            "converged": bool(r3["converged"])}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -370,6 +404,7 @@ def run_ours(args):
             "gpu_launches": int(launches) * args.steps,
             "clocks": clk,
             "scf": scf,
+            "mixed": mixed,
             "bit_identical_host_vs_device": bit_identical,
             "classes": per_class,
         }
@@ -387,6 +422,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="w32-631gs")
     ap.add_argument("--no-scf", action="store_true")
+    ap.add_argument("--fp32-bound", type=float, default=1e-5,
+                    help="mixed form: FP32 below this Schwarz bound product (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)

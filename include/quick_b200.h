@@ -117,6 +117,14 @@ int qk_schwarz(qk_ctx *ctx, double *YCutoff, double *cutPrim);
 int qk_set_schwarz(qk_ctx *ctx, const double *YCutoff, const double *cutPrim);
 /* integralCutoff and primLimit (src/modules/quick_method_module.f90:772-775). */
 int qk_set_cutoffs(qk_ctx *ctx, double integralCutoff, double primLimit);
+/* Mixed precision (no counterpart in the reference, which is FP64 throughout): quartets
+ * whose Schwarz bound product Y_ij*Y_kl is below fp32_bound evaluate the vertical
+ * recursion and the primitive contraction in FP32; the Boys function, geometry, HRR,
+ * digestion and the fixed-point accumulation stay FP64, as do the high angular
+ * momentum (cooperative) classes.  0 (the default) = plain FP64. */
+int qk_set_precision(qk_ctx *ctx, double fp32_bound);
+/* Shell quartets of the current work lists that run in FP32 (mixed form). */
+int qk_last_work_mixed(qk_ctx *ctx, long long *quartets_fp32);
 
 /* o_dev += G(D_dev).  D_dev, o_dev: nbasis^2 FP64 on the device.  cutmat_dev: nshell^2
  * density screen (max |D| per shell pair) or NULL to derive it from D_dev on the device

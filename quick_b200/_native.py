@@ -21,7 +21,8 @@ EXPORTED = [
     "qk_destroy", "qk_default_ctx", "qk_set_basis", "qk_schwarz", "qk_set_schwarz",
     "qk_set_cutoffs", "qk_fock2e_device", "qk_fock2e_host", "qk_density_cutoff_device",
     "qk_last_work", "qk_launches_per_build", "qk_oei_host", "qk_set_profiling",
-    "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc",
+    "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc", "qk_set_precision",
+    "qk_last_work_mixed",
 ]
 
 _lib = None
@@ -70,6 +71,8 @@ def lib():
     L.qk_fp64_peak.argtypes = [I, ctypes.POINTER(ctypes.c_double)]
     L.qk_fock2e_device_noalloc.argtypes = [P, P, P, P, P]
     L.qk_fock2e_device_noalloc.restype = I
+    L.qk_set_precision.argtypes = [P, D]
+    L.qk_last_work_mixed.argtypes = [P, ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTED:
         if name.startswith("gpu_"):
             getattr(L, name).restype = None

@@ -84,16 +84,19 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Contracted [e0|f0] over the primitive pairs of a bra and a ket pair.
-// acc[f*NE + e]; prim_screen applies QUICK's primitive cutoff.
-template <int La, int Lb, int Lc, int Ld>
+// acc[f*NE + e]; prim_screen applies QUICK's primitive cutoff.  R is the type of
+// the vertical recursion and of acc: double for the plain path, float for the
+// small-bound quartets of the mixed form.  Geometry and the Boys function are
+// always evaluated in FP64 and rounded to R afterwards.
+template <int La, int Lb, int Lc, int Ld, typename R = double>
 __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int bnp, int bps, int kp0, int knp,
                                                  int kps,
                                                  const double C[3], double dnmax, bool prim_screen,
-                                                 double* acc, int* nprim_done) {
+                                                 R* acc, int* nprim_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int M = Cls::M;
 #pragma unroll
-    for (int i = 0; i < Cls::NE * Cls::NF; ++i) acc[i] = 0.0;
+    for (int i = 0; i < Cls::NE * Cls::NF; ++i) acc[i] = R(0);
     for (int i = 0; i < bnp; ++i) {
         const int pi = bp0 + i * bps;
         const double zeta = __ldg(d.pp_zeta + pi);
@@ -118,17 +121,20 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
             const double pref = Kab * __ldg(d.pp_K + pj) * rs;
             double F[M + 1];
             boys_scaled<M>(T, pref, d.boys, F);
-            VrrGeom<double> G;
-            G.PA[0] = PAx; G.PA[1] = PAy; G.PA[2] = PAz;
-            G.WP[0] = -rho_z * PQx; G.WP[1] = -rho_z * PQy; G.WP[2] = -rho_z * PQz;
-            G.QC[0] = Qx - C[0]; G.QC[1] = Qy - C[1]; G.QC[2] = Qz - C[2];
-            G.WQ[0] = rho_e * PQx; G.WQ[1] = rho_e * PQy; G.WQ[2] = rho_e * PQz;
-            G.oo2z = oo2z;
-            G.oo2e = __ldg(d.pp_oo2z + pj);
-            G.oo2ze = 0.5 * inv_s;
-            G.rho_z = rho_z;
-            G.rho_e = rho_e;
-            Cls::template vrr<double>(F, G, acc);
+            VrrGeom<R> G;
+            G.PA[0] = R(PAx); G.PA[1] = R(PAy); G.PA[2] = R(PAz);
+            G.WP[0] = R(-rho_z * PQx); G.WP[1] = R(-rho_z * PQy); G.WP[2] = R(-rho_z * PQz);
+            G.QC[0] = R(Qx - C[0]); G.QC[1] = R(Qy - C[1]); G.QC[2] = R(Qz - C[2]);
+            G.WQ[0] = R(rho_e * PQx); G.WQ[1] = R(rho_e * PQy); G.WQ[2] = R(rho_e * PQz);
+            G.oo2z = R(oo2z);
+            G.oo2e = R(__ldg(d.pp_oo2z + pj));
+            G.oo2ze = R(0.5 * inv_s);
+            G.rho_z = R(rho_z);
+            G.rho_e = R(rho_e);
+            R Fr[M + 1];
+#pragma unroll
+            for (int m = 0; m <= M; ++m) Fr[m] = R(F[m]);
+            Cls::template vrr<R>(Fr, G, acc);
         }
     }
 }
@@ -137,8 +143,8 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
 // Lane-private updates go straight to A; the bra J block is returned in jab
 // (already weighted) for the warp reduction.
 template <int La, int Lb, int Lc, int Ld>
-__device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, double* jab_out, int* nq_done,
-                                             int* np_done) {
+__device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, bool fp32, double* jab_out,
+                                             int* nq_done, int* np_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND;
     constexpr int NE = Cls::NE, NF = Cls::NF, NAB = NA * NB;
@@ -160,8 +166,17 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, dou
     const double CD[3] = {Cc[0] - d.xyz[3 * id], Cc[1] - d.xyz[3 * id + 1], Cc[2] - d.xyz[3 * id + 2]};
 
     double acc[NE * NF];
-    contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q],
-                                     d.pr_pps[Q], Cc, dnmax, true, acc, np_done);
+    if (fp32) {
+        // mixed form: small-bound quartet, vertical recursion and contraction in FP32
+        float accf[NE * NF];
+        contract_quartet<La, Lb, Lc, Ld, float>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q],
+                                                d.pr_npp[Q], d.pr_pps[Q], Cc, dnmax, true, accf, np_done);
+#pragma unroll
+        for (int i = 0; i < NE * NF; ++i) acc[i] = (double)accf[i];
+    } else {
+        contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q],
+                                         d.pr_pps[Q], Cc, dnmax, true, acc, np_done);
+    }
 
     // bra HRR per ket column
     double t1[NF * NAB];
@@ -489,7 +504,8 @@ fock_coop_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __
     }
 }
 
-// Work item: x = bra pair, y = first ket pair, z = number of kets (<= 32).
+// Work item: x = bra pair, y = first ket pair, z = number of kets (<= 32),
+// w = 1 for the mixed form's FP32 quartets.
 template <int La, int Lb, int Lc, int Ld>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
 fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __restrict__ counter) {
@@ -506,7 +522,7 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, jab, &nq, &np);
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
         if (d.stats) {
             const unsigned sq = __reduce_add_sync(0xffffffffu, (unsigned)nq);
             const unsigned sp = __reduce_add_sync(0xffffffffu, (unsigned)np);
@@ -808,7 +824,7 @@ constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
 struct ClassWork {
     std::vector<int4> items;
     DevBuf<int4> d_items;
-    long long nquart = 0, nprimq = 0;
+    long long nquart = 0, nprimq = 0, nquart32 = 0;
     int grid = 0;
 };
 
@@ -826,6 +842,8 @@ struct qk_ctx {
     bool have_basis = false, have_schwarz = false;
     std::vector<double> Ycut, cutprim;   // nshell^2, jbasis^2 (symmetric)
     double integralCutoff = 1e-7, primLimit = 1e-8;
+    double fp32_bound = 0.0;          // mixed form: FP32 below this Schwarz bound product
+    double built_fp32 = -1.0;
     double built_cut = -1.0;
     bool pairs_dirty = true;
     qk::PairTable pairs;
@@ -1056,7 +1074,7 @@ static int build_work(qk_ctx* c) {
         const ClassEntry& ce = g_classes[ci];
         ClassWork& W = c->work[ci];
         W.items.clear();
-        W.nquart = W.nprimq = 0;
+        W.nquart = W.nprimq = W.nquart32 = 0;
         const bool same = (ce.La == ce.Lc && ce.Lb == ce.Ld);
         struct Tmp { int4 it; long long cost; };
         std::vector<Tmp> tmp;
@@ -1085,8 +1103,22 @@ static int build_work(qk_ctx* c) {
                     // (one quartet per warp at a time): one ket per item, so that the
                     // few, long quartets spread over many warps
                     const int chunk = ce.coop ? 1 : 32;
-                    for (int s = 0; s < nk; s += chunk)
-                        tmp.push_back({make_int4(P, K.begin + s, std::min(chunk, nk - s), 0), cost});
+                    // mixed form: kets with yp * yq below fp32_bound (a suffix, Y sorted
+                    // descending) go to FP32 items; the cooperative classes stay FP64
+                    int n64 = nk;
+                    if (c->fp32_bound > 0.0 && !ce.coop) {
+                        int a = 0, z = nk;
+                        while (a < z) {
+                            const int mid = (a + z) / 2;
+                            if (yp * T.Y[K.begin + mid] >= c->fp32_bound) a = mid + 1; else z = mid;
+                        }
+                        n64 = a;
+                    }
+                    W.nquart32 += nk - n64;
+                    for (int s = 0; s < n64; s += chunk)
+                        tmp.push_back({make_int4(P, K.begin + s, std::min(chunk, n64 - s), 0), cost});
+                    for (int s = n64; s < nk; s += chunk)
+                        tmp.push_back({make_int4(P, K.begin + s, std::min(chunk, nk - s), 1), cost});
                 }
             }
         }
@@ -1129,7 +1161,7 @@ static int build_work(qk_ctx* c) {
 static int ensure_pairs(qk_ctx* c) {
     if (!c->have_basis) return fail(QK_ERR_NOT_READY, "basis not uploaded");
     if (!c->have_schwarz) return fail(QK_ERR_NOT_READY, "Schwarz bounds not set");
-    if (!c->pairs_dirty && c->built_cut == c->integralCutoff) return QK_OK;
+    if (!c->pairs_dirty && c->built_cut == c->integralCutoff && c->built_fp32 == c->fp32_bound) return QK_OK;
     build_pairs(c, true);
     int st = upload_pairs(c);
     if (st) return st;
@@ -1138,6 +1170,7 @@ static int ensure_pairs(qk_ctx* c) {
     // tables were uploaded on the context stream; builds may run on another stream
     QK_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->built_cut = c->integralCutoff;
+    c->built_fp32 = c->fp32_bound;
     c->pairs_dirty = false;
     return QK_OK;
 }
@@ -1568,6 +1601,21 @@ int qk_set_cutoffs(qk_ctx* c, double integralCutoff, double primLimit) {
     std::lock_guard<std::mutex> g(c->mu);
     c->integralCutoff = integralCutoff;
     c->primLimit = primLimit;
+    return QK_OK;
+}
+
+int qk_set_precision(qk_ctx* c, double fp32_bound) {
+    if (!c || !(fp32_bound >= 0.0)) return fail(QK_ERR_INVALID_ARG, "bad precision bound");
+    std::lock_guard<std::mutex> g(c->mu);
+    c->fp32_bound = fp32_bound;
+    return QK_OK;
+}
+
+int qk_last_work_mixed(qk_ctx* c, long long* quartets_fp32) {
+    if (!c || !quartets_fp32) return fail(QK_ERR_INVALID_ARG, "null argument");
+    long long q = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci) q += c->work[ci].nquart32;
+    *quartets_fp32 = q;
     return QK_OK;
 }
 

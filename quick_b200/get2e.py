@@ -86,6 +86,17 @@ class Get2e:
         self.Ycut, self.cutprim = _f64(Y), _f64(cutprim)
         check(lib().qk_set_schwarz(self.h, _p(self.Ycut), _p(self.cutprim)), "qk_set_schwarz")
 
+    def set_precision(self, fp32_bound: float):
+        """Mixed form: FP32 vertical recursion for quartets with Y_ij*Y_kl < fp32_bound
+        (0 = plain FP64)."""
+        self.fp32_bound = float(fp32_bound)
+        check(lib().qk_set_precision(self.h, self.fp32_bound), "qk_set_precision")
+
+    def fp32_quartets(self):
+        q = ctypes.c_longlong(0)
+        check(lib().qk_last_work_mixed(self.h, ctypes.byref(q)), "qk_last_work_mixed")
+        return q.value
+
     def set_cutoffs(self, integral_cutoff: float, prim_limit: float):
         self.integral_cutoff, self.prim_limit = float(integral_cutoff), float(prim_limit)
         check(lib().qk_set_cutoffs(self.h, self.integral_cutoff, self.prim_limit), "qk_set_cutoffs")
