@@ -156,6 +156,19 @@ int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_de
 int qk_fock2e_device_noalloc(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
                              double *o_dev, void *stream);
 
+/* ------------------------------------------------------------- batches
+ * Many molecules in one Fock build (no counterpart in the reference, which builds one
+ * molecule per process): for every class one merged work list over all molecules,
+ * launched once, so that small molecules fill the GPU together.  Each context keeps
+ * its own tables, cutoffs and precision; o_dev[m] += G(D_dev[m]) for every molecule.
+ * cutmat_dev may be NULL (or hold NULL entries) to screen from D on the device.  The
+ * merged lists are cached and rebuilt when the set of contexts or their lists change. */
+typedef struct qk_batch qk_batch;
+qk_batch *qk_batch_create(int device, int *status);
+int qk_batch_destroy(qk_batch *batch);
+int qk_batch_fock2e(qk_batch *batch, int n, qk_ctx *const *ctx, const double *const *D_dev,
+                    const double *const *cutmat_dev, double *const *o_dev, void *stream);
+
 /* Work statistics of the last build: shell quartets listed and primitive quartets
  * listed after Schwarz screening (before density screening). */
 int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int *launches);

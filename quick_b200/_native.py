@@ -22,7 +22,7 @@ EXPORTED = [
     "qk_set_cutoffs", "qk_fock2e_device", "qk_fock2e_host", "qk_density_cutoff_device",
     "qk_last_work", "qk_launches_per_build", "qk_oei_host", "qk_set_profiling",
     "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc", "qk_set_precision",
-    "qk_last_work_mixed",
+    "qk_last_work_mixed", "qk_batch_create", "qk_batch_destroy", "qk_batch_fock2e",
 ]
 
 _lib = None
@@ -73,6 +73,10 @@ def lib():
     L.qk_fock2e_device_noalloc.restype = I
     L.qk_set_precision.argtypes = [P, D]
     L.qk_last_work_mixed.argtypes = [P, ctypes.POINTER(ctypes.c_longlong)]
+    L.qk_batch_create.restype = P
+    L.qk_batch_create.argtypes = [I, PI]
+    L.qk_batch_destroy.argtypes = [P]
+    L.qk_batch_fock2e.argtypes = [P, I, P, P, P, P, P]
     for name in EXPORTED:
         if name.startswith("gpu_"):
             getattr(L, name).restype = None

@@ -543,6 +543,62 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
     }
 }
 
+
+// Batched (many-molecule) variants: one launch per class walks a merged work
+// list of every molecule's items; the item's w holds (molecule << 1) | fp32 and
+// the molecule's device data comes from dl[molecule].
+template <int La, int Lb, int Lc, int Ld>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+fock_class_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__ items, int n_items,
+                        int* __restrict__ counter) {
+    using Cls = EriClass<La, Lb, Lc, Ld>;
+    constexpr int NAB = Cls::NA * Cls::NB;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const DevData& d = dl[w.w >> 1];
+        double jab[NAB];
+#pragma unroll
+        for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
+        int nq = 0, np = 0;
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, (w.w & 1) != 0, jab, &nq, &np);
+        const int P = w.x;
+        const int fa = d.q_f0[d.pr_qa[P]], fb = d.q_f0[d.pr_qb[P]];
+#pragma unroll
+        for (int i = 0; i < NAB; ++i) {
+            const double s = warp_sum(jab[i]);
+            if (lane == 0 && s != 0.0)
+                atomic_fixed(d.A + (size_t)(fa + i / Cls::NB) * d.nbasis + fb + i % Cls::NB, s);
+        }
+    }
+}
+
+template <int La, int Lb, int Lc, int Ld>
+__global__ void __launch_bounds__(32 * kCoopWarps)
+fock_coop_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__ items, int n_items,
+                       int* __restrict__ counter) {
+    using Lay = CoopLayout<La, Lb, Lc, Ld>;
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* acc = smem + (size_t)warp * Lay::PER_WARP;
+    double* V = acc + Lay::ACC;
+    double* Db = V + Lay::WORK;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const DevData& d = dl[w.w >> 1];
+        int nq = 0, np = 0;
+        for (int k = 0; k < w.z; ++k) coop_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + k, acc, V, Db, lane, &nq, &np);
+    }
+}
+
 // Schwarz bounds: one thread per (pair, mode); mode < 0 = contracted (ab|ab),
 // mode = k = primitive-pair diagonal quartet of primitive pair k.  Writes
 // max |(ab|ab)| (with QUICK's cons factors) through an unsigned atomicMax on the
@@ -790,6 +846,22 @@ const void* fock_fn_ptr() {
     else
         return (const void*)&fock_class_kernel<a, b, c, e>;
 }
+using FockBatchFn = void (*)(dim3, dim3, size_t, cudaStream_t, const DevData*, const int4*, int, int*);
+template <int a, int b, int c, int e>
+void launch_fock_batch(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData* dl, const int4* it, int n,
+                       int* cnt) {
+    if constexpr (EriClass<a, b, c, e>::COOP)
+        fock_coop_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, it, n, cnt);
+    else
+        fock_class_kernel_batch<a, b, c, e><<<g, bl, 0, s>>>(dl, it, n, cnt);
+}
+template <int a, int b, int c, int e>
+const void* fock_batch_fn_ptr() {
+    if constexpr (EriClass<a, b, c, e>::COOP)
+        return (const void*)&fock_coop_kernel_batch<a, b, c, e>;
+    else
+        return (const void*)&fock_class_kernel_batch<a, b, c, e>;
+}
 template <int a, int b, int c, int e>
 constexpr size_t coop_smem() {
     if constexpr (EriClass<a, b, c, e>::COOP)
@@ -806,6 +878,8 @@ struct ClassEntry {
     bool coop;                          // one quartet per warp (high angular momentum)
     size_t smem;                        // dynamic shared memory of a block (coop only)
     int coop_warps;                     // warps per block of the cooperative kernel
+    FockBatchFn fn_batch;               // many-molecule variant
+    const void* (*kernel_batch)();
 };
 template <int a, int b, int c, int e>
 constexpr int coop_warps() {
@@ -816,13 +890,15 @@ constexpr int coop_warps() {
 }
 #define QK_X(a, b, c, e) {a, b, c, e, &launch_fock<a, b, c, e>, &fock_fn_ptr<a, b, c, e>, \
                           EriClass<a, b, c, e>::PRIM_FLOPS, EriClass<a, b, c, e>::QUARTET_FLOPS, \
-                          EriClass<a, b, c, e>::COOP, coop_smem<a, b, c, e>(), coop_warps<a, b, c, e>()},
+                          EriClass<a, b, c, e>::COOP, coop_smem<a, b, c, e>(), coop_warps<a, b, c, e>(), \
+                          &launch_fock_batch<a, b, c, e>, &fock_batch_fn_ptr<a, b, c, e>},
 static const ClassEntry g_classes[] = {QK_ERI_CLASS_LIST(QK_X)};
 #undef QK_X
 constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
 
 struct ClassWork {
     std::vector<int4> items;
+    std::vector<long long> cost;   // per item, for merging lists of several molecules
     DevBuf<int4> d_items;
     long long nquart = 0, nprimq = 0, nquart32 = 0;
     int grid = 0;
@@ -843,6 +919,7 @@ struct qk_ctx {
     std::vector<double> Ycut, cutprim;   // nshell^2, jbasis^2 (symmetric)
     double integralCutoff = 1e-7, primLimit = 1e-8;
     double fp32_bound = 0.0;          // mixed form: FP32 below this Schwarz bound product
+    unsigned long long work_version = 0;   // bumped whenever the work lists are rebuilt
     double built_fp32 = -1.0;
     double built_cut = -1.0;
     bool pairs_dirty = true;
@@ -919,6 +996,13 @@ static double cons_expected(const int c[3]) {
         return std::sqrt(5.0) * std::sqrt(3.0);
     }
     return 1.0;
+}
+
+// Work-list versions are unique across all contexts of the process, so that a
+// batch never mistakes a new context at a freed context's address for the old one.
+static unsigned long long next_work_version() {
+    static std::atomic<unsigned long long> counter{0};
+    return ++counter;
 }
 
 static DevData make_devdata(qk_ctx* c) {
@@ -1124,7 +1208,11 @@ static int build_work(qk_ctx* c) {
         }
         std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) { return x.cost > y.cost; });
         W.items.resize(tmp.size());
-        for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
+        W.cost.resize(tmp.size());
+        for (size_t i = 0; i < tmp.size(); ++i) {
+            W.items[i] = tmp[i].it;
+            W.cost[i] = tmp[i].cost;
+        }
         QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
         if (!W.items.empty()) {
             const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
@@ -1139,6 +1227,7 @@ static int build_work(qk_ctx* c) {
         }
     }
     c->launches += 1;  // finalize
+    c->work_version = next_work_version();
     c->launch_order.clear();
     for (int ci = 0; ci < kNumClasses; ++ci)
         if (!c->work[ci].items.empty()) c->launch_order.push_back(ci);
@@ -1346,6 +1435,82 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
         }
     finalize_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(A, n, o);
     QK_CUDA_TRY(cudaGetLastError());
+    return QK_OK;
+}
+
+}  // namespace qk
+
+
+// ------------------------------------------------------------------ batches
+// Many molecules in one Fock build: per class one merged work list over all
+// molecules (items tagged with their molecule, ordered by cost), launched once.
+struct qk_batch {
+    int device = 0;
+    std::mutex mu;
+    int num_sms = 148;
+    std::vector<qk_ctx*> key;                       // molecules of the cached lists
+    std::vector<unsigned long long> key_version;
+    qk::ClassWork work[qk::kNumClasses];
+    std::vector<int> launch_order;
+    qk::DevBuf<qk::DevData> d_dl;
+    qk::DevBuf<int> d_counters;
+    static constexpr int kAux = 4;
+    cudaStream_t aux[kAux] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
+};
+
+namespace qk {
+
+static int batch_merge(qk_batch* b, int n, qk_ctx* const* ctxs) {
+    bool same = (int)b->key.size() == n;
+    for (int i = 0; same && i < n; ++i)
+        same = b->key[i] == ctxs[i] && b->key_version[i] == ctxs[i]->work_version;
+    if (same) return QK_OK;
+    b->launch_order.clear();
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        const ClassEntry& ce = g_classes[ci];
+        ClassWork& W = b->work[ci];
+        struct Tmp { int4 it; long long cost; };
+        std::vector<Tmp> tmp;
+        W.nquart = W.nprimq = W.nquart32 = 0;
+        for (int m = 0; m < n; ++m) {
+            const ClassWork& S = ctxs[m]->work[ci];
+            for (size_t k = 0; k < S.items.size(); ++k) {
+                int4 it = S.items[k];
+                it.w = (m << 1) | (it.w & 1);
+                tmp.push_back({it, S.cost[k]});
+            }
+            W.nquart += S.nquart;
+            W.nprimq += S.nprimq;
+        }
+        std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) { return x.cost > y.cost; });
+        W.items.resize(tmp.size());
+        for (size_t k = 0; k < tmp.size(); ++k) W.items[k] = tmp[k].it;
+        QK_CUDA_TRY(W.d_items.upload(W.items, nullptr));
+        W.grid = 0;
+        if (!W.items.empty()) {
+            const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
+            if (ce.smem > 48 * 1024)
+                QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel_batch(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)ce.smem));
+            int bps = 0;
+            QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel_batch(), 32 * wpb, ce.smem));
+            if (bps < 1) return fail(QK_ERR_CUDA, "batched class kernel cannot be resident");
+            const long long need = ((long long)W.items.size() + wpb - 1) / wpb;
+            W.grid = (int)std::min<long long>((long long)bps * b->num_sms, need);
+            b->launch_order.push_back(ci);
+        }
+    }
+    std::stable_sort(b->launch_order.begin(), b->launch_order.end(), [&](int x, int y) {
+        if (g_classes[x].coop != g_classes[y].coop) return g_classes[x].coop;
+        const double wx = b->work[x].nprimq * g_classes[x].prim_flops + b->work[x].nquart * g_classes[x].quartet_flops;
+        const double wy = b->work[y].nprimq * g_classes[y].prim_flops + b->work[y].nquart * g_classes[y].quartet_flops;
+        return wx > wy;
+    });
+    QK_CUDA_TRY(cudaDeviceSynchronize());   // item uploads finished before they are read
+    b->key.assign(ctxs, ctxs + n);
+    b->key_version.resize(n);
+    for (int i = 0; i < n; ++i) b->key_version[i] = ctxs[i]->work_version;
     return QK_OK;
 }
 
@@ -1676,6 +1841,110 @@ int qk_fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutmat, d
     std::lock_guard<std::mutex> g(c->mu);
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
     return fock2e_device_noalloc(c, D, cutmat, o, (cudaStream_t)stream);
+}
+
+
+// ------------------------------------------------------------- batches (C ABI)
+qk_batch* qk_batch_create(int device, int* status) {
+    if (cudaSetDevice(device) != cudaSuccess) {
+        if (status) *status = fail(QK_ERR_NO_DEVICE, "qk_batch_create: cudaSetDevice");
+        return nullptr;
+    }
+    qk_batch* b = new qk_batch();
+    b->device = device;
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
+    bool ok = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; ok && k < qk_batch::kAux; ++k)
+        ok = cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok || b->d_counters.reserve(kNumClasses) != cudaSuccess) {
+        qk_batch_destroy(b);
+        if (status) *status = fail(QK_ERR_CUDA, "qk_batch_create");
+        return nullptr;
+    }
+    if (status) *status = QK_OK;
+    return b;
+}
+
+int qk_batch_destroy(qk_batch* b) {
+    if (!b) return QK_OK;
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    for (auto& a : b->aux)
+        if (a) cudaStreamDestroy(a);
+    for (auto& e : b->join_ev)
+        if (e) cudaEventDestroy(e);
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    delete b;
+    return QK_OK;
+}
+
+int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const* D, const double* const* cutmat,
+                    double* const* o, void* stream) {
+    if (!b || n <= 0 || !ctxs || !D || !o) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: null argument");
+    if (n > (1 << 20)) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: too many molecules");
+    std::lock_guard<std::mutex> g(b->mu);
+    if (cudaSetDevice(b->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<DevData> h((size_t)n);
+    for (int m = 0; m < n; ++m) {
+        qk_ctx* c = ctxs[m];
+        if (!c || !D[m] || !o[m]) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: null molecule entry");
+        if (c->device != b->device) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: context on another device");
+        for (int j = 0; j < m; ++j)
+            if (ctxs[j] == c)
+                return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: a context appears twice (its accumulator is shared)");
+        std::lock_guard<std::mutex> gc(c->mu);
+        int st = ensure_pairs(c);
+        if (st) return st;
+        const int nb = c->nbasis, ns = c->nshell;
+        const double* cm = cutmat ? cutmat[m] : nullptr;
+        if (!cm) {
+            QK_CUDA_TRY(c->d_cutmat.reserve((size_t)ns * ns));
+            density_cutoff_kernel<<<(ns * ns + 127) / 128, 128, 0, s>>>(D[m], nb, ns, c->d_shell_f0.p,
+                                                                         c->d_shell_f1.p, c->d_cutmat.p);
+            QK_CUDA_TRY(cudaGetLastError());
+            cm = c->d_cutmat.p;
+        }
+        QK_CUDA_TRY(c->d_A.reserve((size_t)nb * nb));
+        QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * nb * nb, s));
+        h[m] = make_devdata(c);
+        h[m].D = D[m];
+        h[m].cutmat = cm;
+        h[m].A = c->d_A.p;
+        h[m].stats = nullptr;
+    }
+    int st = batch_merge(b, n, ctxs);
+    if (st) return st;
+    QK_CUDA_TRY(b->d_dl.reserve((size_t)n));
+    QK_CUDA_TRY(cudaMemcpyAsync(b->d_dl.p, h.data(), sizeof(DevData) * n, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaMemsetAsync(b->d_counters.p, 0, sizeof(int) * kNumClasses, s));
+    QK_CUDA_TRY(cudaEventRecord(b->fork_ev, s));
+    bool used[qk_batch::kAux] = {};
+    int slot = 0;
+    for (int ci : b->launch_order) {
+        const ClassWork& W = b->work[ci];
+        const int k = slot++ % qk_batch::kAux;
+        if (!used[k]) {
+            QK_CUDA_TRY(cudaStreamWaitEvent(b->aux[k], b->fork_ev, 0));
+            used[k] = true;
+        }
+        const ClassEntry& ce = g_classes[ci];
+        ce.fn_batch(dim3(W.grid), dim3(32 * (ce.coop ? ce.coop_warps : kWarpsPerBlock)), ce.smem, b->aux[k],
+                    b->d_dl.p, W.d_items.p, (int)W.items.size(), b->d_counters.p + ci);
+        QK_CUDA_TRY(cudaGetLastError());
+    }
+    for (int k = 0; k < qk_batch::kAux; ++k)
+        if (used[k]) {
+            QK_CUDA_TRY(cudaEventRecord(b->join_ev[k], b->aux[k]));
+            QK_CUDA_TRY(cudaStreamWaitEvent(s, b->join_ev[k], 0));
+        }
+    for (int m = 0; m < n; ++m) {
+        const int nb = ctxs[m]->nbasis;
+        finalize_kernel<<<(nb * nb + 255) / 256, 256, 0, s>>>(h[m].A, nb, o[m]);
+        QK_CUDA_TRY(cudaGetLastError());
+    }
+    return QK_OK;
 }
 
 int qk_last_work(qk_ctx* c, long long* quartets, long long* primq, int* launches) {

@@ -154,6 +154,67 @@ class Get2e:
         return {"quartets": q.value, "prim_quartets": pq.value, "launches": nl.value}
 
 
+class Get2eBatch:
+    """Fock builds of many molecules at once on one GPU (``qk_batch_*``).
+
+    Every molecule keeps its own :class:`Get2e` context (basis, Schwarz bounds,
+    cutoffs, precision); one call builds ``o[m] += G(D[m])`` for all of them with
+    one launch per integral class over the merged work lists, so that molecules
+    too small to fill the GPU alone share it.  Results equal the one-molecule
+    builds bit for bit (same quartets, same int64 accumulation)."""
+
+    def __init__(self, device: int = 0):
+        st = _c_int(0)
+        self.h = lib().qk_batch_create(int(device), ctypes.byref(st))
+        if not self.h:
+            raise QuickError(st.value, "qk_batch_create")
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().qk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def fock2e(self, engines, Ds, os=None, cutmats=None, stream=None):
+        """o[m] += G(D[m]) for every engine m; tensors are CUDA float64.
+
+        Returns the list of o tensors (zeros allocated where not given).
+        Enqueued on ``stream`` (default: torch's current stream)."""
+        import torch
+        n = len(engines)
+        if n == 0:
+            return []
+        if len(Ds) != n:
+            raise ValueError("one density per engine")
+        Ds = [D.contiguous() for D in Ds]
+        if os is None:
+            os = [None] * n
+        os = list(os)
+        for m, (e, D) in enumerate(zip(engines, Ds)):
+            nb = e.basis.nbasis
+            if D.dtype != torch.float64 or not D.is_cuda or tuple(D.shape) != (nb, nb):
+                raise ValueError(f"D[{m}] must be a CUDA float64 tensor of shape ({nb}, {nb})")
+            if os[m] is None:
+                os[m] = torch.zeros((nb, nb), dtype=torch.float64, device=D.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(Ds[0].device)
+        VP = ctypes.c_void_p
+        hs = (VP * n)(*[e.h for e in engines])
+        dp = (VP * n)(*[D.data_ptr() for D in Ds])
+        op = (VP * n)(*[o.data_ptr() for o in os])
+        cp = None
+        if cutmats is not None:
+            cp = (VP * n)(*[c.data_ptr() if c is not None else None for c in cutmats])
+        check(lib().qk_batch_fock2e(self.h, n, hs, dp, cp, op, VP(stream.cuda_stream)), "qk_batch_fock2e")
+        return os
+
+
 # ---------------------------------------------------------------------------
 # The reference's Fortran -> C call sequence (all arguments by reference).
 # ---------------------------------------------------------------------------
