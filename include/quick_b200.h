@@ -156,6 +156,15 @@ int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_de
 int qk_fock2e_device_noalloc(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
                              double *o_dev, void *stream);
 
+/* Build the shell-pair tables and work lists for the current basis, Schwarz bounds,
+ * cutoffs and precision now (the first Fock build does it otherwise), e.g. while
+ * other work keeps the GPU busy.  Uses only the context's own stream. */
+int qk_prepare(qk_ctx *ctx);
+
+/* Device memory held by a context (pair tables, work lists, accumulators), in bytes;
+ * *items = the part taken by the work lists (a batch holds one more copy of them). */
+int qk_device_bytes(qk_ctx *ctx, unsigned long long *total, unsigned long long *items);
+
 /* ------------------------------------------------------------- batches
  * Many molecules in one Fock build (no counterpart in the reference, which builds one
  * molecule per process): for every class one merged work list over all molecules,

@@ -23,6 +23,7 @@ EXPORTED = [
     "qk_last_work", "qk_launches_per_build", "qk_oei_host", "qk_set_profiling",
     "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc", "qk_set_precision",
     "qk_last_work_mixed", "qk_batch_create", "qk_batch_destroy", "qk_batch_fock2e",
+    "qk_device_bytes", "qk_prepare",
 ]
 
 _lib = None
@@ -77,6 +78,8 @@ def lib():
     L.qk_batch_create.argtypes = [I, PI]
     L.qk_batch_destroy.argtypes = [P]
     L.qk_batch_fock2e.argtypes = [P, I, P, P, P, P, P]
+    L.qk_prepare.argtypes = [P]
+    L.qk_device_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
     for name in EXPORTED:
         if name.startswith("gpu_"):
             getattr(L, name).restype = None

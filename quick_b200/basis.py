@@ -121,12 +121,9 @@ class Molecule:
 
     def nuclear_repulsion(self) -> float:
         """Ecore without external charges (src/getEnergy.f90:68-84)."""
-        e = 0.0
-        for i in range(self.natom):
-            for j in range(i + 1, self.natom):
-                r = math.sqrt(float(((self.xyz[i] - self.xyz[j]) ** 2).sum()))
-                e += float(self.Z[i]) * float(self.Z[j]) / r
-        return e
+        i, j = np.triu_indices(self.natom, 1)
+        r = np.sqrt(((self.xyz[i] - self.xyz[j]) ** 2).sum(axis=1))
+        return float((self.Z[i].astype(np.float64) * self.Z[j] / r).sum())
 
 
 @dataclass

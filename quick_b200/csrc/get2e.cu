@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -544,12 +545,31 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
 }
 
 
-// Batched (many-molecule) variants: one launch per class walks a merged work
-// list of every molecule's items; the item's w holds (molecule << 1) | fp32 and
-// the molecule's device data comes from dl[molecule].
+// Batched (many-molecule) variants.  Per class, the work of every molecule stays
+// in that molecule's own item list; a segment table (one entry per molecule with
+// work in the class: its list, the prefix count of items before it, its index)
+// joins them into one virtual list that the warps walk with one atomic counter.
+// A warp finds the segment of its item by binary search over the prefix counts
+// (a few cached loads, shared by the warp) -- nothing is copied or re-sorted
+// when molecules join or leave the batch.
+struct BatchSeg {
+    const int4* items;
+    int begin;   // items of the class before this segment
+    int mol;     // index into the batch's DevData array
+};
+
+__device__ __forceinline__ int batch_find_seg(const BatchSeg* __restrict__ segs, int nseg, int it) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].begin <= it) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <int La, int Lb, int Lc, int Ld>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
-fock_class_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__ items, int n_items,
+fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restrict__ segs, int nseg, int n_items,
                         int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NAB = Cls::NA * Cls::NB;
@@ -559,13 +579,14 @@ fock_class_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__
         if (lane == 0) it = atomicAdd(counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= n_items) break;
-        const int4 w = items[it];
-        const DevData& d = dl[w.w >> 1];
+        const BatchSeg sg = segs[batch_find_seg(segs, nseg, it)];
+        const int4 w = sg.items[it - sg.begin];
+        const DevData& d = dl[sg.mol];
         double jab[NAB];
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, (w.w & 1) != 0, jab, &nq, &np);
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
         const int P = w.x;
         const int fa = d.q_f0[d.pr_qa[P]], fb = d.q_f0[d.pr_qb[P]];
 #pragma unroll
@@ -579,7 +600,7 @@ fock_class_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__
 
 template <int La, int Lb, int Lc, int Ld>
 __global__ void __launch_bounds__(32 * kCoopWarps)
-fock_coop_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__ items, int n_items,
+fock_coop_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restrict__ segs, int nseg, int n_items,
                        int* __restrict__ counter) {
     using Lay = CoopLayout<La, Lb, Lc, Ld>;
     extern __shared__ double smem[];
@@ -592,10 +613,52 @@ fock_coop_kernel_batch(const DevData* __restrict__ dl, const int4* __restrict__ 
         if (lane == 0) it = atomicAdd(counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= n_items) break;
-        const int4 w = items[it];
-        const DevData& d = dl[w.w >> 1];
+        const BatchSeg sg = segs[batch_find_seg(segs, nseg, it)];
+        const int4 w = sg.items[it - sg.begin];
+        const DevData& d = dl[sg.mol];
         int nq = 0, np = 0;
         for (int k = 0; k < w.z; ++k) coop_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + k, acc, V, Db, lane, &nq, &np);
+    }
+}
+
+// Per-molecule set-up and finish of a batched build, one launch each for all
+// molecules: grid (chunks, molecules), grid-stride inside a molecule.
+struct BatchMol {
+    const double* D;
+    double* cut;                  // density screen to compute here, or null (caller's)
+    unsigned long long* A;
+    double* o;
+    const int* s_f0;
+    const int* s_f1;
+    int n, ns;
+};
+
+__global__ void batch_prep_kernel(const BatchMol* __restrict__ ml) {
+    const BatchMol m = ml[blockIdx.y];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nn = (long long)m.n * m.n;
+    for (long long t = t0; t < nn; t += stride) m.A[t] = 0ull;
+    if (m.cut) {
+        const long long ns2 = (long long)m.ns * m.ns;
+        for (long long t = t0; t < ns2; t += stride) {
+            const int a = (int)(t / m.ns), b = (int)(t % m.ns);
+            double v = 0.0;
+            for (int i = m.s_f0[a]; i < m.s_f1[a]; ++i)
+                for (int j = m.s_f0[b]; j < m.s_f1[b]; ++j) v = fmax(v, fabs(m.D[(size_t)j * m.n + i]));
+            m.cut[t] = v;
+        }
+    }
+}
+
+__global__ void batch_finalize_kernel(const BatchMol* __restrict__ ml) {
+    const BatchMol m = ml[blockIdx.y];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long nn = (long long)m.n * m.n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += stride) {
+        const int i = (int)(t / m.n), j = (int)(t % m.n);
+        const long long v = (long long)(m.A[(size_t)i * m.n + j] + m.A[(size_t)j * m.n + i]);
+        m.o[t] += (double)v * kFixedInv;
     }
 }
 
@@ -796,6 +859,7 @@ struct DevBuf {
         if (e == cudaSuccess) cap = count;
         return e;
     }
+    size_t bytes() const { return cap * sizeof(T); }
     cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
         cudaError_t e = reserve(v.size());
         if (e != cudaSuccess || v.empty()) return e;
@@ -846,14 +910,14 @@ const void* fock_fn_ptr() {
     else
         return (const void*)&fock_class_kernel<a, b, c, e>;
 }
-using FockBatchFn = void (*)(dim3, dim3, size_t, cudaStream_t, const DevData*, const int4*, int, int*);
+using FockBatchFn = void (*)(dim3, dim3, size_t, cudaStream_t, const DevData*, const BatchSeg*, int, int, int*);
 template <int a, int b, int c, int e>
-void launch_fock_batch(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData* dl, const int4* it, int n,
-                       int* cnt) {
+void launch_fock_batch(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData* dl, const BatchSeg* segs,
+                       int nseg, int n, int* cnt) {
     if constexpr (EriClass<a, b, c, e>::COOP)
-        fock_coop_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, it, n, cnt);
+        fock_coop_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
     else
-        fock_class_kernel_batch<a, b, c, e><<<g, bl, 0, s>>>(dl, it, n, cnt);
+        fock_class_kernel_batch<a, b, c, e><<<g, bl, 0, s>>>(dl, segs, nseg, n, cnt);
 }
 template <int a, int b, int c, int e>
 const void* fock_batch_fn_ptr() {
@@ -898,7 +962,6 @@ constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
 
 struct ClassWork {
     std::vector<int4> items;
-    std::vector<long long> cost;   // per item, for merging lists of several molecules
     DevBuf<int4> d_items;
     long long nquart = 0, nprimq = 0, nquart32 = 0;
     int grid = 0;
@@ -1208,11 +1271,7 @@ static int build_work(qk_ctx* c) {
         }
         std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) { return x.cost > y.cost; });
         W.items.resize(tmp.size());
-        W.cost.resize(tmp.size());
-        for (size_t i = 0; i < tmp.size(); ++i) {
-            W.items[i] = tmp[i].it;
-            W.cost[i] = tmp[i].cost;
-        }
+        for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
         QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
         if (!W.items.empty()) {
             const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
@@ -1442,79 +1501,30 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
 
 
 // ------------------------------------------------------------------ batches
-// Many molecules in one Fock build: per class one merged work list over all
-// molecules (items tagged with their molecule, ordered by cost), launched once.
+// Many molecules in one Fock build.  Per call the host writes one staging block
+// -- the molecules' DevData, their BatchMol records and every class's segment
+// table -- into pinned memory (two blocks, used in turn, each guarded by the
+// event of its last copy), copies it to the device with one cudaMemcpyAsync, and
+// enqueues: counters memset, batch_prep_kernel, the class kernels (forked over
+// auxiliary streams), batch_finalize_kernel.
 struct qk_batch {
     int device = 0;
     std::mutex mu;
     int num_sms = 148;
-    std::vector<qk_ctx*> key;                       // molecules of the cached lists
-    std::vector<unsigned long long> key_version;
-    qk::ClassWork work[qk::kNumClasses];
-    std::vector<int> launch_order;
-    qk::DevBuf<qk::DevData> d_dl;
+    int bps[qk::kNumClasses] = {};            // resident blocks per SM of each batched class kernel
+    static constexpr int kStage = 2;
+    char* h_stage[kStage] = {};
+    size_t h_cap[kStage] = {};
+    cudaEvent_t stage_ev[kStage] = {};
+    int stage_next = 0;
+    qk::DevBuf<char> d_stage;
     qk::DevBuf<int> d_counters;
+    cudaEvent_t done_ev = nullptr;            // end of the previous build (orders reuse of d_stage)
+    bool done_recorded = false;
     static constexpr int kAux = 4;
     cudaStream_t aux[kAux] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
 };
-
-namespace qk {
-
-static int batch_merge(qk_batch* b, int n, qk_ctx* const* ctxs) {
-    bool same = (int)b->key.size() == n;
-    for (int i = 0; same && i < n; ++i)
-        same = b->key[i] == ctxs[i] && b->key_version[i] == ctxs[i]->work_version;
-    if (same) return QK_OK;
-    b->launch_order.clear();
-    for (int ci = 0; ci < kNumClasses; ++ci) {
-        const ClassEntry& ce = g_classes[ci];
-        ClassWork& W = b->work[ci];
-        struct Tmp { int4 it; long long cost; };
-        std::vector<Tmp> tmp;
-        W.nquart = W.nprimq = W.nquart32 = 0;
-        for (int m = 0; m < n; ++m) {
-            const ClassWork& S = ctxs[m]->work[ci];
-            for (size_t k = 0; k < S.items.size(); ++k) {
-                int4 it = S.items[k];
-                it.w = (m << 1) | (it.w & 1);
-                tmp.push_back({it, S.cost[k]});
-            }
-            W.nquart += S.nquart;
-            W.nprimq += S.nprimq;
-        }
-        std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) { return x.cost > y.cost; });
-        W.items.resize(tmp.size());
-        for (size_t k = 0; k < tmp.size(); ++k) W.items[k] = tmp[k].it;
-        QK_CUDA_TRY(W.d_items.upload(W.items, nullptr));
-        W.grid = 0;
-        if (!W.items.empty()) {
-            const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
-            if (ce.smem > 48 * 1024)
-                QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel_batch(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)ce.smem));
-            int bps = 0;
-            QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel_batch(), 32 * wpb, ce.smem));
-            if (bps < 1) return fail(QK_ERR_CUDA, "batched class kernel cannot be resident");
-            const long long need = ((long long)W.items.size() + wpb - 1) / wpb;
-            W.grid = (int)std::min<long long>((long long)bps * b->num_sms, need);
-            b->launch_order.push_back(ci);
-        }
-    }
-    std::stable_sort(b->launch_order.begin(), b->launch_order.end(), [&](int x, int y) {
-        if (g_classes[x].coop != g_classes[y].coop) return g_classes[x].coop;
-        const double wx = b->work[x].nprimq * g_classes[x].prim_flops + b->work[x].nquart * g_classes[x].quartet_flops;
-        const double wy = b->work[y].nprimq * g_classes[y].prim_flops + b->work[y].nquart * g_classes[y].quartet_flops;
-        return wx > wy;
-    });
-    QK_CUDA_TRY(cudaDeviceSynchronize());   // item uploads finished before they are read
-    b->key.assign(ctxs, ctxs + n);
-    b->key_version.resize(n);
-    for (int i = 0; i < n; ++i) b->key_version[i] = ctxs[i]->work_version;
-    return QK_OK;
-}
-
-}  // namespace qk
 
 using namespace qk;
 
@@ -1853,10 +1863,22 @@ qk_batch* qk_batch_create(int device, int* status) {
     qk_batch* b = new qk_batch();
     b->device = device;
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
-    bool ok = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    bool ok = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->done_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; ok && k < qk_batch::kStage; ++k)
+        ok = cudaEventCreateWithFlags(&b->stage_ev[k], cudaEventDisableTiming) == cudaSuccess;
     for (int k = 0; ok && k < qk_batch::kAux; ++k)
         ok = cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming) == cudaSuccess;
+    for (int ci = 0; ok && ci < kNumClasses; ++ci) {
+        const ClassEntry& ce = g_classes[ci];
+        const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
+        if (ce.smem > 48 * 1024)
+            ok = cudaFuncSetAttribute(ce.kernel_batch(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ce.smem) == cudaSuccess;
+        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->bps[ci], ce.kernel_batch(), 32 * wpb,
+                                                                 ce.smem) == cudaSuccess && b->bps[ci] >= 1;
+    }
     if (!ok || b->d_counters.reserve(kNumClasses) != cudaSuccess) {
         qk_batch_destroy(b);
         if (status) *status = fail(QK_ERR_CUDA, "qk_batch_create");
@@ -1874,19 +1896,29 @@ int qk_batch_destroy(qk_batch* b) {
         if (a) cudaStreamDestroy(a);
     for (auto& e : b->join_ev)
         if (e) cudaEventDestroy(e);
+    for (int k = 0; k < qk_batch::kStage; ++k) {
+        if (b->stage_ev[k]) cudaEventDestroy(b->stage_ev[k]);
+        if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
+    }
     if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    if (b->done_ev) cudaEventDestroy(b->done_ev);
     delete b;
     return QK_OK;
+}
+
+namespace {
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 }
 
 int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const* D, const double* const* cutmat,
                     double* const* o, void* stream) {
     if (!b || n <= 0 || !ctxs || !D || !o) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: null argument");
-    if (n > (1 << 20)) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: too many molecules");
+    if (n > 65535) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: more than 65535 molecules");
     std::lock_guard<std::mutex> g(b->mu);
     if (cudaSetDevice(b->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
     cudaStream_t s = (cudaStream_t)stream;
-    std::vector<DevData> h((size_t)n);
+    // per molecule: tables ready, accumulator and screen buffers sized
+    long long max_nn = 0;
     for (int m = 0; m < n; ++m) {
         qk_ctx* c = ctxs[m];
         if (!c || !D[m] || !o[m]) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: null molecule entry");
@@ -1897,53 +1929,142 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
         std::lock_guard<std::mutex> gc(c->mu);
         int st = ensure_pairs(c);
         if (st) return st;
-        const int nb = c->nbasis, ns = c->nshell;
-        const double* cm = cutmat ? cutmat[m] : nullptr;
-        if (!cm) {
-            QK_CUDA_TRY(c->d_cutmat.reserve((size_t)ns * ns));
-            density_cutoff_kernel<<<(ns * ns + 127) / 128, 128, 0, s>>>(D[m], nb, ns, c->d_shell_f0.p,
-                                                                         c->d_shell_f1.p, c->d_cutmat.p);
-            QK_CUDA_TRY(cudaGetLastError());
-            cm = c->d_cutmat.p;
-        }
-        QK_CUDA_TRY(c->d_A.reserve((size_t)nb * nb));
-        QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * nb * nb, s));
-        h[m] = make_devdata(c);
-        h[m].D = D[m];
-        h[m].cutmat = cm;
-        h[m].A = c->d_A.p;
-        h[m].stats = nullptr;
+        QK_CUDA_TRY(c->d_A.reserve((size_t)c->nbasis * c->nbasis));
+        if (!(cutmat && cutmat[m])) QK_CUDA_TRY(c->d_cutmat.reserve((size_t)c->nshell * c->nshell));
+        max_nn = std::max<long long>(max_nn, (long long)c->nbasis * c->nbasis);
     }
-    int st = batch_merge(b, n, ctxs);
-    if (st) return st;
-    QK_CUDA_TRY(b->d_dl.reserve((size_t)n));
-    QK_CUDA_TRY(cudaMemcpyAsync(b->d_dl.p, h.data(), sizeof(DevData) * n, cudaMemcpyHostToDevice, s));
+    // staging block: [DevData x n][BatchMol x n][BatchSeg per class, classes in order]
+    int seg_count[kNumClasses], seg_off[kNumClasses], total_items[kNumClasses];
+    int nseg_all = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        seg_off[ci] = nseg_all;
+        seg_count[ci] = 0;
+        long long tot = 0;
+        for (int m = 0; m < n; ++m)
+            if (!ctxs[m]->work[ci].items.empty()) {
+                ++seg_count[ci];
+                tot += (long long)ctxs[m]->work[ci].items.size();
+            }
+        if (tot > INT_MAX) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: too many work items in one class");
+        total_items[ci] = (int)tot;
+        nseg_all += seg_count[ci];
+    }
+    const size_t off_mol = align16(sizeof(DevData) * n);
+    const size_t off_seg = off_mol + align16(sizeof(BatchMol) * n);
+    const size_t bytes = off_seg + sizeof(BatchSeg) * (size_t)std::max(nseg_all, 1);
+    const int k = b->stage_next;
+    b->stage_next = (k + 1) % qk_batch::kStage;
+    QK_CUDA_TRY(cudaEventSynchronize(b->stage_ev[k]));   // its previous copy has been read
+    if (b->h_cap[k] < bytes) {
+        if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
+        b->h_stage[k] = nullptr;
+        b->h_cap[k] = 0;
+        QK_CUDA_TRY(cudaHostAlloc((void**)&b->h_stage[k], bytes * 2, cudaHostAllocDefault));
+        b->h_cap[k] = bytes * 2;
+    }
+    char* hs = b->h_stage[k];
+    DevData* hd = (DevData*)hs;
+    BatchMol* hm = (BatchMol*)(hs + off_mol);
+    BatchSeg* hg = (BatchSeg*)(hs + off_seg);
+    for (int m = 0; m < n; ++m) {
+        qk_ctx* c = ctxs[m];
+        const bool own_cut = !(cutmat && cutmat[m]);
+        DevData d = make_devdata(c);
+        d.D = D[m];
+        d.cutmat = own_cut ? c->d_cutmat.p : cutmat[m];
+        d.A = c->d_A.p;
+        d.stats = nullptr;
+        hd[m] = d;
+        hm[m] = BatchMol{D[m], own_cut ? c->d_cutmat.p : nullptr, c->d_A.p, o[m], c->d_shell_f0.p,
+                         c->d_shell_f1.p, c->nbasis, c->nshell};
+    }
+    // device addresses of the staged arrays (d_stage may grow: wait for the last build first)
+    if (b->done_recorded) QK_CUDA_TRY(cudaStreamWaitEvent(s, b->done_ev, 0));
+    if (b->d_stage.cap < bytes) {
+        if (b->done_recorded) QK_CUDA_TRY(cudaEventSynchronize(b->done_ev));
+        QK_CUDA_TRY(b->d_stage.reserve(bytes * 2));
+    }
+    char* ds = b->d_stage.p;
+    const DevData* dd = (const DevData*)ds;
+    const BatchMol* dm = (const BatchMol*)(ds + off_mol);
+    const BatchSeg* dg = (const BatchSeg*)(ds + off_seg);
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        BatchSeg* sg = hg + seg_off[ci];
+        int at = 0, ns = 0;
+        for (int m = 0; m < n; ++m) {
+            const ClassWork& W = ctxs[m]->work[ci];
+            if (W.items.empty()) continue;
+            sg[ns++] = BatchSeg{W.d_items.p, at, m};
+            at += (int)W.items.size();
+        }
+    }
+    QK_CUDA_TRY(cudaMemcpyAsync(ds, hs, bytes, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaEventRecord(b->stage_ev[k], s));
     QK_CUDA_TRY(cudaMemsetAsync(b->d_counters.p, 0, sizeof(int) * kNumClasses, s));
+    const int chunks = (int)std::min<long long>(64, std::max<long long>(1, (max_nn + 2047) / 2048));
+    batch_prep_kernel<<<dim3(chunks, n), 256, 0, s>>>(dm);
+    QK_CUDA_TRY(cudaGetLastError());
+    // class launches, cooperative (long) classes first, then by total items
+    int order[kNumClasses], no = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci)
+        if (total_items[ci] > 0) order[no++] = ci;
+    std::stable_sort(order, order + no, [&](int x, int y) {
+        if (g_classes[x].coop != g_classes[y].coop) return g_classes[x].coop;
+        return (double)total_items[x] * g_classes[x].prim_flops > (double)total_items[y] * g_classes[y].prim_flops;
+    });
     QK_CUDA_TRY(cudaEventRecord(b->fork_ev, s));
     bool used[qk_batch::kAux] = {};
-    int slot = 0;
-    for (int ci : b->launch_order) {
-        const ClassWork& W = b->work[ci];
-        const int k = slot++ % qk_batch::kAux;
-        if (!used[k]) {
-            QK_CUDA_TRY(cudaStreamWaitEvent(b->aux[k], b->fork_ev, 0));
-            used[k] = true;
-        }
+    for (int i = 0; i < no; ++i) {
+        const int ci = order[i];
         const ClassEntry& ce = g_classes[ci];
-        ce.fn_batch(dim3(W.grid), dim3(32 * (ce.coop ? ce.coop_warps : kWarpsPerBlock)), ce.smem, b->aux[k],
-                    b->d_dl.p, W.d_items.p, (int)W.items.size(), b->d_counters.p + ci);
-        QK_CUDA_TRY(cudaGetLastError());
-    }
-    for (int k = 0; k < qk_batch::kAux; ++k)
-        if (used[k]) {
-            QK_CUDA_TRY(cudaEventRecord(b->join_ev[k], b->aux[k]));
-            QK_CUDA_TRY(cudaStreamWaitEvent(s, b->join_ev[k], 0));
+        const int a = i % qk_batch::kAux;
+        if (!used[a]) {
+            QK_CUDA_TRY(cudaStreamWaitEvent(b->aux[a], b->fork_ev, 0));
+            used[a] = true;
         }
-    for (int m = 0; m < n; ++m) {
-        const int nb = ctxs[m]->nbasis;
-        finalize_kernel<<<(nb * nb + 255) / 256, 256, 0, s>>>(h[m].A, nb, o[m]);
+        const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
+        const long long need = ((long long)total_items[ci] + wpb - 1) / wpb;
+        const int grid = (int)std::min<long long>((long long)b->bps[ci] * b->num_sms, need);
+        ce.fn_batch(dim3(grid), dim3(32 * wpb), ce.smem, b->aux[a], dd, dg + seg_off[ci], seg_count[ci],
+                    total_items[ci], b->d_counters.p + ci);
         QK_CUDA_TRY(cudaGetLastError());
     }
+    for (int a = 0; a < qk_batch::kAux; ++a)
+        if (used[a]) {
+            QK_CUDA_TRY(cudaEventRecord(b->join_ev[a], b->aux[a]));
+            QK_CUDA_TRY(cudaStreamWaitEvent(s, b->join_ev[a], 0));
+        }
+    batch_finalize_kernel<<<dim3(chunks, n), 256, 0, s>>>(dm);
+    QK_CUDA_TRY(cudaGetLastError());
+    QK_CUDA_TRY(cudaEventRecord(b->done_ev, s));
+    b->done_recorded = true;
+    return QK_OK;
+}
+
+int qk_prepare(qk_ctx* c) {
+    if (!c) return fail(QK_ERR_INVALID_ARG, "qk_prepare: null context");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    return ensure_pairs(c);
+}
+
+int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* items) {
+    if (!c) return fail(QK_ERR_INVALID_ARG, "qk_device_bytes: null context");
+    std::lock_guard<std::mutex> g(c->mu);
+    const PairTable& T = c->pairs;
+    unsigned long long it = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci) it += c->work[ci].d_items.bytes();
+    unsigned long long t = it;
+    for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
+                     T.d_Y.bytes(), T.d_zeta.bytes(), T.d_oo2z.bytes(), T.d_K.bytes(), T.d_cut.bytes(),
+                     T.d_Px.bytes(), T.d_Py.bytes(), T.d_Pz.bytes(), T.d_PAx.bytes(), T.d_PAy.bytes(),
+                     T.d_PAz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
+                     c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(),
+                     c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
+                     c->d_A.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
+        t += b;
+    if (total) *total = t;
+    if (items) *items = it;
     return QK_OK;
 }
 

@@ -6,10 +6,13 @@
 // src/gpu/gpu_oei.h:193) for closed-shell SCF set-up.  Integrals use the
 // McMurchie-Davidson Hermite expansion over QUICK's normalize_basis
 // representation (aexp/dcoeff/itype/ncenter, src/modules/quick_basis_module.f90:385-424).
-// One thread per basis-function pair (mu >= nu); results are symmetric.
+// One thread per basis-function pair (mu >= nu) and chunk of point charges;
+// results are symmetric and bit-reproducible.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "quick_b200.h"
@@ -34,6 +37,16 @@ struct OeiArgs {
     const double* boys;
     double *S, *T, *V;     // nbasis^2
 };
+
+// Flat index of (t, u, v) among the triples with t + u + v <= 2 * kOeiLmax,
+// ordered by total degree, then t descending, then u descending.
+constexpr int kTuvMax = (2 * kOeiLmax + 1) * (2 * kOeiLmax + 2) * (2 * kOeiLmax + 3) / 6;
+__device__ __forceinline__ int tuv_index(int t, int u, int v) {
+    const int L = t + u + v;
+    const int before = L * (L + 1) * (L + 2) / 6;           // triples of lower degree
+    const int r = L - t;                                     // u + v
+    return before + r * (r + 1) / 2 + v;
+}
 
 // 1-D Hermite coefficients E[i][j][t], i <= li, j <= lj, for one Cartesian axis.
 __device__ __forceinline__ void hermite_E(int li, int lj, double XPA, double XPB, double oo2p, double E0,
@@ -65,10 +78,16 @@ __device__ __forceinline__ void hermite_E(int li, int lj, double XPA, double XPB
     }
 }
 
-__global__ void oei_kernel(OeiArgs a) {
+// grid (pairs / 128, charge chunks): chunk y sums the attraction of charges
+// [y * chunk, (y + 1) * chunk) into Vpart[y][pair]; chunk 0 also writes S and T.
+__global__ void oei_kernel(OeiArgs a, int chunk, double* __restrict__ Vpart) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = a.nbasis;
-    if (t >= n * (n + 1) / 2) return;
+    const int npair = n * (n + 1) / 2;
+    if (t >= npair) return;
+    const int c0 = blockIdx.y * chunk;
+    const int c1 = min(a.ncharge, c0 + chunk);
+    const bool first = blockIdx.y == 0;
     // t -> (mu, nu), mu >= nu
     int mu = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
     while (mu * (mu + 1) / 2 > t) --mu;
@@ -107,53 +126,100 @@ __global__ void oei_kernel(OeiArgs a) {
             const double cc = ca * cb;
             s += cc * S1[0] * S1[1] * S1[2];
             tk += cc * (T1[0] * S1[1] * S1[2] + S1[0] * T1[1] * S1[2] + S1[0] * S1[1] * T1[2]);
-            // nuclear attraction: (2 pi / p) sum_tuv E_t E_u E_v R_tuv
+            // nuclear attraction: (2 pi / p) sum_tuv E_t E_u E_v R_tuv, with the
+            // Hermite Coulomb integrals R built level by level (k = Lsum .. 0) in
+            // two flat arrays over t + u + v <= Lsum - k
             const double pref = cc * 2.0 * M_PI / pz;
-            for (int c = 0; c < a.ncharge; ++c) {
+            const int lx = la[0] + lb[0], ly = la[1] + lb[1], lz = la[2] + lb[2];
+            double Ex[2 * kOeiLmax + 1], Ey[2 * kOeiLmax + 1], Ez[2 * kOeiLmax + 1];
+            for (int q2 = 0; q2 <= 2 * kOeiLmax; ++q2) {
+                Ex[q2] = q2 <= lx ? E[0][la[0]][lb[0]][q2] : 0.0;
+                Ey[q2] = q2 <= ly ? E[1][la[1]][lb[1]][q2] : 0.0;
+                Ez[q2] = q2 <= lz ? E[2][la[2]][lb[2]][q2] : 0.0;
+            }
+            double m2p[2 * kOeiLmax + 1];   // (-2p)^k
+            m2p[0] = 1.0;
+            for (int k = 1; k <= 2 * kOeiLmax; ++k) m2p[k] = m2p[k - 1] * (-2.0 * pz);
+            for (int c = c0; c < c1; ++c) {
                 const double PC[3] = {P[0] - a.cxyz[3 * c], P[1] - a.cxyz[3 * c + 1], P[2] - a.cxyz[3 * c + 2]};
                 const double r2 = PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2];
                 double F[2 * kOeiLmax + 1];
                 boys_scaled<2 * kOeiLmax>(pz * r2, 1.0, a.boys, F);
-                // R[n][t][u][v], n + t + u + v <= Lsum
-                double R[2 * kOeiLmax + 1][2 * kOeiLmax + 1][2 * kOeiLmax + 1][2 * kOeiLmax + 1];
-                double m2p = 1.0;
-                for (int k = 0; k <= Lsum; ++k) {
-                    R[k][0][0][0] = m2p * F[k];
-                    m2p *= -2.0 * pz;
-                }
+                double Ra[kTuvMax], Rb[kTuvMax];
+                double* Rn = Ra;   // level k + 1
+                double* Rc = Rb;   // level k
+                Rn[0] = m2p[Lsum] * F[Lsum];
                 for (int k = Lsum - 1; k >= 0; --k) {
-                    const int L = Lsum - k;   // t+u+v <= L at level k
+                    const int L = Lsum - k;
+                    Rc[0] = m2p[k] * F[k];
                     for (int tt = 0; tt <= L; ++tt)
                         for (int uu = 0; uu <= L - tt; ++uu)
                             for (int vv = 0; vv <= L - tt - uu; ++vv) {
                                 if (tt + uu + vv == 0) continue;
                                 double r;
                                 if (tt > 0) {
-                                    r = PC[0] * R[k + 1][tt - 1][uu][vv];
-                                    if (tt > 1) r += (tt - 1) * R[k + 1][tt - 2][uu][vv];
+                                    r = PC[0] * Rn[tuv_index(tt - 1, uu, vv)];
+                                    if (tt > 1) r += (tt - 1) * Rn[tuv_index(tt - 2, uu, vv)];
                                 } else if (uu > 0) {
-                                    r = PC[1] * R[k + 1][tt][uu - 1][vv];
-                                    if (uu > 1) r += (uu - 1) * R[k + 1][tt][uu - 2][vv];
+                                    r = PC[1] * Rn[tuv_index(tt, uu - 1, vv)];
+                                    if (uu > 1) r += (uu - 1) * Rn[tuv_index(tt, uu - 2, vv)];
                                 } else {
-                                    r = PC[2] * R[k + 1][tt][uu][vv - 1];
-                                    if (vv > 1) r += (vv - 1) * R[k + 1][tt][uu][vv - 2];
+                                    r = PC[2] * Rn[tuv_index(tt, uu, vv - 1)];
+                                    if (vv > 1) r += (vv - 1) * Rn[tuv_index(tt, uu, vv - 2)];
                                 }
-                                R[k][tt][uu][vv] = r;
+                                Rc[tuv_index(tt, uu, vv)] = r;
                             }
+                    double* tmp = Rn; Rn = Rc; Rc = tmp;
                 }
+                // Rn holds level 0
                 double vc = 0.0;
-                for (int tt = 0; tt <= la[0] + lb[0]; ++tt)
-                    for (int uu = 0; uu <= la[1] + lb[1]; ++uu)
-                        for (int vv = 0; vv <= la[2] + lb[2]; ++vv)
-                            vc += E[0][la[0]][lb[0]][tt] * E[1][la[1]][lb[1]][uu] * E[2][la[2]][lb[2]][vv] *
-                                  R[0][tt][uu][vv];
+                for (int tt = 0; tt <= lx; ++tt)
+                    for (int uu = 0; uu <= ly; ++uu)
+                        for (int vv = 0; vv <= lz; ++vv) vc += Ex[tt] * Ey[uu] * Ez[vv] * Rn[tuv_index(tt, uu, vv)];
                 v -= a.cq[c] * pref * vc;
             }
         }
     }
-    a.S[(size_t)mu * n + nu] = s; a.S[(size_t)nu * n + mu] = s;
-    a.T[(size_t)mu * n + nu] = tk; a.T[(size_t)nu * n + mu] = tk;
-    a.V[(size_t)mu * n + nu] = v; a.V[(size_t)nu * n + mu] = v;
+    if (first) {
+        a.S[(size_t)mu * n + nu] = s; a.S[(size_t)nu * n + mu] = s;
+        a.T[(size_t)mu * n + nu] = tk; a.T[(size_t)nu * n + mu] = tk;
+    }
+    Vpart[(size_t)blockIdx.y * npair + t] = v;
+}
+
+// V = sum of the chunks' partial sums, in chunk order (bit-reproducible).
+__global__ void oei_reduce_kernel(OeiArgs a, int nchunk, const double* __restrict__ Vpart) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = a.nbasis;
+    const int npair = n * (n + 1) / 2;
+    if (t >= npair) return;
+    int mu = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while (mu * (mu + 1) / 2 > t) --mu;
+    while ((mu + 1) * (mu + 2) / 2 <= t) ++mu;
+    const int nu = t - mu * (mu + 1) / 2;
+    double v = 0.0;
+    for (int k = 0; k < nchunk; ++k) v += Vpart[(size_t)k * npair + t];
+    a.V[(size_t)mu * n + nu] = v;
+    a.V[(size_t)nu * n + mu] = v;
+}
+
+// One non-blocking stream per device for the one-electron set-up, so that it
+// neither waits for nor holds up work on other streams (no device-wide syncs:
+// stream-ordered allocation, copies and a stream synchronisation only).
+static cudaStream_t oei_stream(int device) {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    std::lock_guard<std::mutex> g(mu);
+    if (device < 0 || device >= 64) return nullptr;
+    if (!streams[device]) cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking);
+    return streams[device];
+}
+
+static const std::vector<double>& oei_boys_table() {
+    static std::once_flag once;
+    static std::vector<double> tab;
+    std::call_once(once, [] { tab = boys_table(); });
+    return tab;
 }
 
 }  // namespace qk
@@ -182,35 +248,50 @@ extern "C" int qk_oei_host(int device, int natom, const double* xyz, const doubl
         for (int k = 0; k < 3; ++k) cxyz[3 * (natom + i) + k] = ext_xyz[3 * i + k];
         cq[natom + i] = ext_q[i];
     }
-    std::vector<double> tab = boys_table();
+    const std::vector<double>& tab = oei_boys_table();
     const size_t nn = (size_t)nbasis * nbasis;
-    void* bufs[11] = {};
-    size_t sizes[11] = {nbasis * sizeof(int), 3 * nbasis * sizeof(int), (size_t)maxcontract * nbasis * 8,
+    const long long npair = (long long)nbasis * (nbasis + 1) / 2;
+    // charge chunks: enough blocks for about 4 waves of the GPU, at least 32 charges a chunk
+    const long long want = std::max<long long>(1, (4LL * 148 * 2048 + npair - 1) / npair);
+    const int nchunk = (int)std::max<long long>(1, std::min<long long>({want, (nq + 31) / 32, 65535LL}));
+    const int chunk = (nq + nchunk - 1) / nchunk;
+    cudaStream_t s = oei_stream(device);
+    if (!s) return QK_ERR_CUDA;
+    // one device block: inputs, then S T V, then the partial sums
+    size_t sizes[10] = {nbasis * sizeof(int), 3 * nbasis * sizeof(int), (size_t)maxcontract * nbasis * 8,
                         (size_t)maxcontract * nbasis * 8, nbasis * sizeof(int), 3 * (size_t)natom * 8,
-                        cxyz.size() * 8, cq.size() * 8, tab.size() * 8, 3 * nn * 8, 0};
-    const void* src[10] = {ncontract, itype, aexp, dcoeff, ncenter, xyz, cxyz.data(), cq.data(), tab.data(), nullptr};
+                        cxyz.size() * 8, cq.size() * 8, tab.size() * 8, 3 * nn * 8};
+    const void* src[9] = {ncontract, itype, aexp, dcoeff, ncenter, xyz, cxyz.data(), cq.data(), tab.data()};
+    size_t off[11];
+    off[0] = 0;
+    for (int i = 0; i < 10; ++i) off[i + 1] = off[i] + ((sizes[i] + 255) & ~size_t(255));
+    const size_t total = off[10] + (size_t)nchunk * npair * 8;
+    char* base = nullptr;
+    if (cudaMallocAsync((void**)&base, total, s) != cudaSuccess) return QK_ERR_OUT_OF_MEMORY;
     int st = QK_OK;
-    for (int i = 0; i < 10 && st == QK_OK; ++i) {
-        if (cudaMalloc(&bufs[i], sizes[i]) != cudaSuccess) { st = QK_ERR_OUT_OF_MEMORY; break; }
-        if (src[i] && cudaMemcpy(bufs[i], src[i], sizes[i], cudaMemcpyHostToDevice) != cudaSuccess) st = QK_ERR_CUDA;
-    }
+    for (int i = 0; i < 9 && st == QK_OK; ++i)
+        if (cudaMemcpyAsync(base + off[i], src[i], sizes[i], cudaMemcpyHostToDevice, s) != cudaSuccess)
+            st = QK_ERR_CUDA;
     if (st == QK_OK) {
         OeiArgs a;
         a.nbasis = nbasis; a.maxcontract = maxcontract; a.ncharge = nq;
-        a.ncontract = (const int*)bufs[0]; a.itype = (const int*)bufs[1];
-        a.aexp = (const double*)bufs[2]; a.dcoeff = (const double*)bufs[3];
-        a.ncenter = (const int*)bufs[4]; a.xyz = (const double*)bufs[5];
-        a.cxyz = (const double*)bufs[6]; a.cq = (const double*)bufs[7]; a.boys = (const double*)bufs[8];
-        a.S = (double*)bufs[9]; a.T = a.S + nn; a.V = a.T + nn;
-        const int npair = nbasis * (nbasis + 1) / 2;
-        oei_kernel<<<(npair + 127) / 128, 128>>>(a);
-        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = QK_ERR_CUDA;
-        if (st == QK_OK && (cudaMemcpy(S, a.S, nn * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                            cudaMemcpy(T, a.T, nn * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                            cudaMemcpy(V, a.V, nn * 8, cudaMemcpyDeviceToHost) != cudaSuccess))
+        a.ncontract = (const int*)(base + off[0]); a.itype = (const int*)(base + off[1]);
+        a.aexp = (const double*)(base + off[2]); a.dcoeff = (const double*)(base + off[3]);
+        a.ncenter = (const int*)(base + off[4]); a.xyz = (const double*)(base + off[5]);
+        a.cxyz = (const double*)(base + off[6]); a.cq = (const double*)(base + off[7]);
+        a.boys = (const double*)(base + off[8]);
+        a.S = (double*)(base + off[9]); a.T = a.S + nn; a.V = a.T + nn;
+        double* Vpart = (double*)(base + off[10]);
+        const int gx = (int)((npair + 127) / 128);
+        oei_kernel<<<dim3(gx, nchunk), 128, 0, s>>>(a, chunk, Vpart);
+        oei_reduce_kernel<<<gx, 128, 0, s>>>(a, nchunk, Vpart);
+        if (cudaGetLastError() != cudaSuccess) st = QK_ERR_CUDA;
+        if (st == QK_OK && (cudaMemcpyAsync(S, a.S, nn * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                            cudaMemcpyAsync(T, a.T, nn * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                            cudaMemcpyAsync(V, a.V, nn * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess))
             st = QK_ERR_CUDA;
     }
-    for (int i = 0; i < 10; ++i)
-        if (bufs[i]) cudaFree(bufs[i]);
+    cudaFreeAsync(base, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) st = QK_ERR_CUDA;
     return st;
 }

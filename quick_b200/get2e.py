@@ -46,8 +46,15 @@ class Get2e:
         self.h = L.qk_create(int(device), ctypes.byref(st))
         if not self.h:
             raise QuickError(st.value, "qk_create")
-        self.basis = basis
         self.device = device
+        self.bind(basis, schwarz)
+        self.set_cutoffs(integral_cutoff, prim_limit)
+
+    def bind(self, basis, schwarz=None):
+        """Put another molecule (or geometry) on this context: the device buffers
+        are kept and grown as needed; Schwarz bounds are recomputed unless given."""
+        L = lib()
+        self.basis = basis
         b = basis
         self._keep = [np.ascontiguousarray(b.xyz, dtype=np.float64), _i32(b.kstart), _i32(b.katom),
                       _i32(b.kprim), _i32(b.ksumtype), _i32(b.qstart), _i32(b.qfinal),
@@ -60,7 +67,6 @@ class Get2e:
             self.Ycut, self.cutprim = self.schwarz()
         else:
             self.set_schwarz(*schwarz)
-        self.set_cutoffs(integral_cutoff, prim_limit)
 
     def close(self):
         if getattr(self, "h", None):
@@ -145,6 +151,17 @@ class Get2e:
             cm = _p(cm_arr)
         check(lib().qk_fock2e_host(self.h, _p(D), cm, _p(out)), "qk_fock2e_host")
         return out
+
+    def prepare(self):
+        """Build the pair tables and work lists now rather than in the first build."""
+        check(lib().qk_prepare(self.h), "qk_prepare")
+
+    def device_bytes(self):
+        """(total, work-list) bytes of device memory held by the context."""
+        t = ctypes.c_ulonglong(0)
+        it = ctypes.c_ulonglong(0)
+        check(lib().qk_device_bytes(self.h, ctypes.byref(t), ctypes.byref(it)), "qk_device_bytes")
+        return t.value, it.value
 
     def work(self):
         q = ctypes.c_longlong(0)

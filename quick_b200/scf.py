@@ -62,11 +62,8 @@ def external_repulsion(mol, ext_charges):
         return 0.0
     pos = np.asarray(ext_charges[0], dtype=np.float64).reshape(-1, 3)
     q = np.asarray(ext_charges[1], dtype=np.float64)
-    e = 0.0
-    for a in range(mol.natom):
-        r = np.linalg.norm(pos - mol.xyz[a], axis=1)
-        e += float(mol.Z[a]) * float((q / r).sum())
-    return e
+    r = np.sqrt(((mol.xyz[:, None, :] - pos[None, :, :]) ** 2).sum(axis=2))
+    return float((mol.Z.astype(np.float64)[:, None] * q[None, :] / r).sum())
 
 
 class RHF:
@@ -106,54 +103,112 @@ class RHF:
         F0 += self.torch.diag(d)
         return self.density(F0)
 
+    def state(self, denserms: float = 1e-6, maxiter: int = 100, guess="gwh", incremental: bool = True,
+              ncyc: int = 3, maxdiis: int = 10, D0=None):
+        """A solve that advances one Fock build at a time (:class:`SCFState`)."""
+        return SCFState(self, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0)
+
     def run(self, denserms: float = 1e-6, maxiter: int = 100, guess="gwh", incremental: bool = True,
             ncyc: int = 3, maxdiis: int = 10, D0=None, verbose=False):
-        torch = self.torch
-        D = D0.clone() if D0 is not None else self.guess(guess)
-        errs, focks = [], []
-        F_prev = D_prev = None
         t0 = time.perf_counter()
-        history = []
-        converged = False
-        for it in range(1, maxiter + 1):
-            if incremental and F_prev is not None and it >= ncyc:
-                F = F_prev.clone()
-                self.eng.fock2e(D - D_prev, o=F)
-            else:
-                F = self.H.clone()
-                self.eng.fock2e(D, o=F)
-            self.fock_builds += 1
-            F_prev, D_prev = F, D
-            Eel = 0.5 * float(torch.sum(D * (self.H + F)))
-            err = F @ D @ self.S - self.S @ D @ F
-            errs.append(self.X.T @ err @ self.X)
-            focks.append(F)
-            if len(errs) > maxdiis:
-                errs.pop(0)
-                focks.pop(0)
-            nd = len(errs)
-            E = torch.stack(errs).reshape(nd, -1)
-            Bm = -torch.ones((nd + 1, nd + 1), dtype=torch.float64, device=self.device)
-            Bm[:nd, :nd] = E @ E.T
-            Bm[nd, nd] = 0.0
-            rhs = torch.zeros(nd + 1, dtype=torch.float64, device=self.device)
-            rhs[nd] = -1.0
-            try:
-                c = torch.linalg.solve(Bm, rhs)[:nd]
-                Fd = torch.einsum("k,kij->ij", c, torch.stack(focks))
-            except RuntimeError:
-                Fd = F
-            Dn = self.density(Fd)
-            dD = Dn - D
-            prms = float(torch.sqrt(torch.mean(dD * dD)))
-            pchange = float(torch.abs(dD).max())
-            history.append((it, Eel + self.Ecore, prms))
+        st = self.state(denserms, maxiter, guess, incremental, ncyc, maxdiis, D0)
+        while not st.done:
+            Db, F = st.fock_input()
+            self.eng.fock2e(Db, o=F)
+            st.step(st.step_device().tolist())
             if verbose:
-                print(it, Eel + self.Ecore, prms, pchange)
-            if it >= 3 and prms < denserms and pchange < 100 * denserms:
-                converged = True
-                break
-            D = Dn
-        torch.cuda.synchronize(self.device)
-        return {"E": Eel + self.Ecore, "Eel": Eel, "Ecore": self.Ecore, "D": D, "F": F, "niter": it,
-                "converged": converged, "seconds": time.perf_counter() - t0, "history": history}
+                print(*st.history[-1])
+        self.torch.cuda.synchronize(self.device)
+        r = st.result()
+        r["seconds"] = time.perf_counter() - t0
+        return r
+
+
+class SCFState:
+    """One RHF solve driven one Fock build at a time, all matrices on the device.
+
+    The loop of :meth:`RHF.run` split at the Fock build, so that a server can
+    advance many solves together with one batched build (``Get2eBatch``) per
+    step and one host synchronisation for all of them:
+
+    1. :meth:`fock_input` -> (density to contract, matrix to accumulate into):
+       D and H on full builds, D - D_prev and F_prev from cycle ``ncyc`` on
+       (QUICK's incremental build, ``quick_scf_operator_module.f90:69-82``);
+    2. the caller adds G(density) into that matrix;
+    3. :meth:`step_device` -> a 3-vector (Eel, PRMS, PCHANGE) on the device:
+       energy, Pulay DIIS over at most ``maxdiis`` vectors
+       (``quick_scf_module.f90:165-802``; a singular DIIS system falls back to
+       the plain Fock matrix on the device, without a host check), and the new
+       density;
+    4. :meth:`step` takes those three numbers on the host and applies QUICK's
+       convergence test (PRMS < denserms and PCHANGE < 100 denserms, at least 3
+       cycles).
+    """
+
+    def __init__(self, rhf, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0):
+        self.rhf = rhf
+        self.torch = rhf.torch
+        self.denserms, self.maxiter = denserms, maxiter
+        self.incremental, self.ncyc, self.maxdiis = incremental, ncyc, maxdiis
+        self.D = D0.clone() if D0 is not None else rhf.guess(guess)
+        self.errs, self.focks = [], []
+        self.F = self.F_prev = self.D_prev = self.Dn = None
+        self.it = 0
+        self.done = False
+        self.converged = False
+        self.Eel = None
+        self.history = []
+
+    def fock_input(self):
+        self.it += 1
+        if self.incremental and self.F_prev is not None and self.it >= self.ncyc:
+            self.F = self.F_prev.clone()
+            return self.D - self.D_prev, self.F
+        self.F = self.rhf.H.clone()
+        return self.D, self.F
+
+    def step_device(self):
+        torch = self.torch
+        r = self.rhf
+        F, D = self.F, self.D
+        r.fock_builds += 1
+        self.F_prev, self.D_prev = F, D
+        Eel = 0.5 * torch.sum(D * (r.H + F))
+        err = F @ D @ r.S - r.S @ D @ F
+        self.errs.append(r.X.T @ err @ r.X)
+        self.focks.append(F)
+        if len(self.errs) > self.maxdiis:
+            self.errs.pop(0)
+            self.focks.pop(0)
+        nd = len(self.errs)
+        E = torch.stack(self.errs).reshape(nd, -1)
+        Bm = -torch.ones((nd + 1, nd + 1), dtype=torch.float64, device=r.device)
+        Bm[:nd, :nd] = E @ E.T
+        Bm[nd, nd] = 0.0
+        rhs = torch.zeros(nd + 1, dtype=torch.float64, device=r.device)
+        rhs[nd] = -1.0
+        sol, info = torch.linalg.solve_ex(Bm, rhs)
+        Fd = torch.einsum("k,kij->ij", sol[:nd], torch.stack(self.focks))
+        ok = (info == 0) & torch.isfinite(Fd).all()
+        Fd = torch.where(ok, Fd, F)
+        self.Dn = r.density(Fd)
+        dD = self.Dn - D
+        return torch.stack([Eel, torch.sqrt(torch.mean(dD * dD)), torch.abs(dD).max()])
+
+    def step(self, vals):
+        Eel, prms, pchange = (float(v) for v in vals)
+        self.Eel = Eel
+        self.history.append((self.it, Eel + self.rhf.Ecore, prms))
+        if self.it >= 3 and prms < self.denserms and pchange < 100 * self.denserms:
+            self.converged = True
+            self.done = True
+        elif self.it >= self.maxiter:
+            self.done = True
+            self.D = self.Dn
+        else:
+            self.D = self.Dn
+
+    def result(self):
+        r = self.rhf
+        return {"E": self.Eel + r.Ecore, "Eel": self.Eel, "Ecore": r.Ecore, "D": self.D, "F": self.F,
+                "niter": self.it, "converged": self.converged, "history": self.history}

@@ -1,0 +1,462 @@
+"""SCF request serving on one GPU around the batched Fock build.
+
+A request is one closed-shell RHF solve: a molecule and a basis, optionally with
+external point charges (a QM/MM step) and a series it belongs to.  The server
+keeps every admitted solve resident on the device -- its :class:`Get2e` context
+(shell-pair tables, work lists, Schwarz bounds), its density, Fock matrices and
+DIIS history -- and advances all of them together: each step is ONE batched
+Fock build over every active molecule (``qk_batch_fock2e``: per integral class
+one launch over the merged work lists of all molecules), followed by each
+solve's DIIS / density update on the device and one host synchronisation for
+the convergence test of all solves.  Solves join and leave between steps
+(continuous batching); a QM/MM repeat starts from the last converged density of
+its series, which stays on the device.
+
+Admission is by a device-memory budget: a request is admitted (first come,
+first served) when the bytes it will hold -- its context (estimated, then
+measured once built) plus its SCF matrices -- fit beside the solves already
+running.  Latency of a request = completion time - arrival
+time; the server reports p50 / p99 beside throughput.
+
+The per-solve arithmetic is :class:`quick_b200.scf.SCFState`, the same object
+``RHF.run`` uses, and a batched Fock build equals the one-molecule build bit
+for bit, so a request's result does not depend on what else was in the batch.
+
+The reference (QUICK) computes one molecule per process and has no server; the
+QM/MM step it serves is the Fortran API's ``get_quick_energy`` call with new
+coordinates and point charges (``src/modules/quick_api_module.f90:373-404``),
+with the previous density reused when ``reusedmx`` is set
+(``quick_api_module.f90:183-291``) -- what a QM/MM repeat stands for here.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .basis import A_TO_BOHRS, Molecule, build_basis
+from .molecules import water_cluster
+
+# TIP3P point charges (e)
+TIP3P_O, TIP3P_H = -0.834, 0.417
+
+
+@dataclass
+class Request:
+    rid: int
+    mol: Molecule
+    basis: str
+    arrival: float = 0.0                 # seconds after the start of the stream
+    ext_charges: tuple = None            # (positions (n, 3) Bohr, charges (n,))
+    series: int = None                   # QM/MM series: warm start from its last density
+    kind: str = "molecule"
+
+
+@dataclass
+class Result:
+    rid: int
+    E: float
+    niter: int
+    converged: bool
+    nbasis: int
+    basis: str
+    kind: str
+    arrival: float
+    admitted: float
+    done: float
+    bytes: int
+    warm: bool = False
+    D: object = field(default=None, repr=False)
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def cluster_box(n: int) -> float:
+    """Cube edge (Angstrom) for an n-water cluster: about the density of the
+    named cluster workloads (4 waters in 6 A, 12 in 8 A, 32 in 10 A)."""
+    return max(6.0, 3.15 * n ** (1.0 / 3.0))
+
+
+def _point_charges(rng, qm_xyz_bohr, n, radius_ang, exclude_ang=2.5):
+    """n TIP3P-type charges (O, H, H, O, ...) uniform in a sphere of ``radius_ang``
+    around the QM centroid, at least ``exclude_ang`` from every QM atom."""
+    c = qm_xyz_bohr.mean(axis=0)
+    R = radius_ang * A_TO_BOHRS
+    ex = exclude_ang * A_TO_BOHRS
+    pos = []
+    while len(pos) < n:
+        v = rng.uniform(-R, R, size=(4 * n, 3))
+        v = v[np.einsum("ij,ij->i", v, v) <= R * R] + c
+        d2 = ((v[:, None, :] - qm_xyz_bohr[None, :, :]) ** 2).sum(-1).min(axis=1)
+        pos.extend(v[d2 >= ex * ex])
+    pos = np.array(pos[:n])
+    q = np.where(np.arange(n) % 3 == 0, TIP3P_O, TIP3P_H)
+    return pos, q
+
+
+def request_stream(n_requests: int, rate: float, seed: int = 20261203, qmmm_fraction: float = 0.25,
+                   max_waters: int = 40, bases=("STO-3G", "6-31G*"), qm_waters: int = 20,
+                   n_charges: int = 4000, charge_radius: float = 15.0, sigma: float = 0.01,
+                   n_series: int = 16):
+    """The serving workload: ``n_requests`` RHF requests with Poisson arrivals at
+    ``rate`` per second.
+
+    * molecules: seeded water clusters with N log-uniform in [1, max_waters]
+      (box from :func:`cluster_box`), basis uniform over ``bases``;
+    * a ``qmmm_fraction`` of requests are QM/MM repeats: ``n_series`` series,
+      each a ``qm_waters`` QM region with ``n_charges`` TIP3P-type point charges
+      within ``charge_radius`` A; every repeat moves the QM atoms and the charges
+      of its series by Gaussian ``sigma`` A (a random walk), and is solved from
+      the series' last density.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    series = []
+    for s in range(n_series):
+        mol = water_cluster(qm_waters, cluster_box(qm_waters), seed=seed + 7919 * (s + 1))
+        pos, q = _point_charges(rng, mol.xyz, n_charges, charge_radius)
+        series.append({"mol": mol, "pos": pos, "q": q, "basis": bases[s % len(bases)]})
+    out = []
+    t = 0.0
+    lo, hi = 0.0, math.log(max_waters)
+    for i in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        if rng.random() < qmmm_fraction:
+            s = int(rng.integers(n_series))
+            S = series[s]
+            sb = sigma * A_TO_BOHRS
+            S["mol"] = Molecule(Z=S["mol"].Z, xyz=S["mol"].xyz + rng.normal(scale=sb, size=S["mol"].xyz.shape))
+            S["pos"] = S["pos"] + rng.normal(scale=sb, size=S["pos"].shape)
+            out.append(Request(i, S["mol"], S["basis"], t, (S["pos"], S["q"]), s, "qmmm"))
+        else:
+            n = int(min(max_waters, max(1, round(math.exp(rng.uniform(lo, hi))))))
+            mol = water_cluster(n, cluster_box(n), seed=int(rng.integers(1 << 31)))
+            out.append(Request(i, mol, bases[int(rng.integers(len(bases)))], t))
+    return out
+
+
+def scf_bytes(nbasis: int, maxdiis: int = 10) -> int:
+    """Device bytes of one solve's SCF matrices: S, H, X, D, D_prev, the new D,
+    F, F_prev, 2 * maxdiis DIIS vectors and about 6 temporaries of the step."""
+    return 8 * nbasis * nbasis * (2 * maxdiis + 14)
+
+
+def context_bytes_estimate(basis) -> int:
+    """Estimate of a context's device bytes before its tables are built: 1 MiB
+    of fixed buffers, 88 bytes per primitive pair, and 400 bytes per nbasis^2
+    for the int64 accumulator, the density screen and the work lists (measured
+    on the water clusters of the serving stream: 130 B/nbasis^2 and less for
+    40 waters).  Replaced by the measured figure after the request's first
+    Fock build."""
+    prims = int(np.asarray(basis.kprim, dtype=np.int64).sum())
+    n = basis.nbasis
+    return (1 << 20) + 88 * prims * prims + 400 * n * n
+
+
+def request_bytes_estimate(basis, maxdiis: int = 10) -> int:
+    """Bytes a request is admitted against before its tables exist."""
+    return context_bytes_estimate(basis) + scf_bytes(basis.nbasis, maxdiis)
+
+
+class _Job:
+    __slots__ = ("req", "eng", "rhf", "st", "bytes", "measured", "admitted", "warm")
+
+
+class Server:
+    """Continuous-batching SCF server on one GPU (see the module docstring).
+
+    ``memory_budget``: device bytes that the admitted solves (and the contexts
+    kept for reuse) may hold; default half of the free device memory at start.
+    ``fp32_bound``: the mixed form's Schwarz bound product below which quartets
+    run in FP32 (0 = plain FP64).  ``max_active``: cap on solves in one batch.
+    ``pool``: retired contexts kept for the next requests (their device buffers
+    are reused by ``Get2e.bind``; allocation and release synchronise the GPU)."""
+
+    def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
+                 denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
+                 max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64):
+        import torch
+        from .get2e import Get2eBatch
+        self.torch = torch
+        self.device = device
+        torch.cuda.set_device(device)
+        if memory_budget is None:
+            free, _ = torch.cuda.mem_get_info(device)
+            memory_budget = free // 2
+        self.budget = int(memory_budget)
+        self.fp32_bound = float(fp32_bound)
+        self.denserms, self.maxiter, self.maxdiis = denserms, maxiter, maxdiis
+        self.integral_cutoff = integral_cutoff
+        self.max_active = max_active
+        self.keep_densities = keep_densities
+        self.pool_max = pool
+        self.pool = []                # (Get2e, bytes) kept for reuse
+        self._arrival = lambda r: r.arrival
+        self.batch = Get2eBatch(device)
+        self.active = []
+        self.queue = deque()
+        self.series_D = {}            # series -> last converged density (device)
+        self.series_busy = set()      # series with a request in flight
+        self.used = 0
+        self.peak_used = 0
+        self.steps = 0
+        self.batch_sizes = []
+        self.rejected = []
+        self.timers = {"admit": 0.0, "setup_engine": 0.0, "setup_rhf": 0.0, "fock": 0.0, "scf": 0.0, "sync": 0.0,
+                       "retire": 0.0, "fock_gpu": 0.0}
+        self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        # set-up of new requests runs on its own stream, beside the batch's builds
+        self.setup_stream = torch.cuda.Stream(device)
+        self.main_stream = torch.cuda.current_stream(device)
+
+    # -- admission
+    def _engine(self, basis):
+        from .get2e import Get2e
+        if self.pool:
+            eng, b = self.pool.pop()
+            self.used -= b
+            eng.bind(basis)
+            return eng
+        eng = Get2e(basis, device=self.device, integral_cutoff=self.integral_cutoff,
+                    prim_limit=0.1 * self.integral_cutoff)
+        if self.fp32_bound > 0.0:
+            eng.set_precision(self.fp32_bound)
+        return eng
+
+    def _setup(self, req, basis, now):
+        from .scf import RHF
+        t = time.perf_counter()
+        eng = self._engine(basis)
+        eng.prepare()
+        t1 = time.perf_counter()
+        with self.torch.cuda.stream(self.setup_stream):
+            rhf = RHF(basis, device=self.device, ext_charges=req.ext_charges, engine=eng)
+            D0 = self.series_D.get(req.series) if req.series is not None else None
+            st = rhf.state(denserms=self.denserms, maxiter=self.maxiter, maxdiis=self.maxdiis, D0=D0)
+        self.timers["setup_engine"] += t1 - t
+        self.timers["setup_rhf"] += time.perf_counter() - t1
+        j = _Job()
+        j.req, j.eng, j.rhf = req, eng, rhf
+        j.warm = D0 is not None
+        j.st = st
+        j.admitted = now
+        j.measured = False
+        return j
+
+    def _admit(self, now):
+        """First come, first served among the admissible requests: a QM/MM repeat
+        waits (without holding up the others) while its series has a request in
+        flight, so that it starts from that request's density."""
+        t = time.perf_counter()
+        skipped = deque()
+        while self.queue and len(self.active) < self.max_active:
+            req = self.queue[0]
+            if req.series is not None and req.series in self.series_busy:
+                skipped.append(self.queue.popleft())
+                continue
+            basis = build_basis(req.mol, req.basis)
+            est = request_bytes_estimate(basis, self.maxdiis)
+            if est > self.budget:
+                self.queue.popleft()
+                self.rejected.append((req.rid, est))
+                continue
+            while self.used + est > self.budget and self.pool:
+                eng, b = self.pool.pop(0)
+                self.used -= b
+                eng.close()
+            if self.used + est > self.budget and self.active:
+                break                      # wait for memory
+            self.queue.popleft()
+            j = self._setup(req, basis, now)
+            j.bytes = est
+            self.used += est
+            self.peak_used = max(self.peak_used, self.used)
+            self.active.append(j)
+            if req.series is not None:
+                self.series_busy.add(req.series)
+        while skipped:
+            self.queue.appendleft(skipped.pop())
+        self.timers["admit"] += time.perf_counter() - t
+
+    # -- one step of every active solve, in two halves: the batched Fock build is
+    # enqueued first, new requests are set up on the host and the side stream
+    # while the GPU computes it, then every solve's DIIS / density update runs
+    # and one host synchronisation reads all convergence figures.
+    def _launch(self):
+        act = self.active
+        t0 = time.perf_counter()
+        ins = [j.st.fock_input() for j in act]
+        self._ev[0].record()
+        self.batch.fock2e([j.eng for j in act], [d for d, _ in ins], os=[f for _, f in ins])
+        self._ev[1].record()
+        self.timers["fock"] += time.perf_counter() - t0
+        return list(act)
+
+    def _finish(self, act, clock):
+        torch = self.torch
+        t1 = time.perf_counter()
+        v = torch.stack([j.st.step_device() for j in act])
+        t2 = time.perf_counter()
+        vals = v.cpu().numpy()
+        t3 = time.perf_counter()
+        self.timers["scf"] += t2 - t1
+        self.timers["sync"] += t3 - t2
+        self.timers["fock_gpu"] += self._ev[0].elapsed_time(self._ev[1]) * 1e-3
+        self.steps += 1
+        self.batch_sizes.append(len(act))
+        done = []
+        ids = {id(j) for j in act}
+        for j, v in zip(act, vals):
+            if not j.measured:
+                tot, _ = j.eng.device_bytes()
+                b = tot + scf_bytes(j.rhf.basis.nbasis, self.maxdiis)
+                self.used += b - j.bytes
+                j.bytes = b
+                j.measured = True
+            j.st.step(v)
+            if j.st.done:
+                done.append(j)
+        self.peak_used = max(self.peak_used, self.used)
+        gone = {id(j) for j in done}
+        self.active = [j for j in self.active if id(j) not in gone]
+        out = []
+        if done:
+            t = clock()
+            for j in done:
+                r = j.st.result()
+                req = j.req
+                if req.series is not None:
+                    self.series_busy.discard(req.series)
+                    if r["converged"]:
+                        self.series_D[req.series] = r["D"]
+                out.append(Result(req.rid, r["E"], r["niter"], r["converged"], j.rhf.basis.nbasis, req.basis,
+                                  req.kind, self._arrival(req), j.admitted, t, j.bytes, j.warm,
+                                  r["D"] if self.keep_densities else None))
+                self.used -= j.bytes
+                if len(self.pool) < self.pool_max:
+                    tot, _ = j.eng.device_bytes()
+                    self.pool.append((j.eng, tot))
+                    self.used += tot
+                else:
+                    j.eng.close()
+        self.timers["retire"] += time.perf_counter() - t3
+        return out
+
+    def serve(self, requests, realtime: bool = True):
+        """Run a request stream to completion; returns the results in request order.
+
+        ``realtime``: requests arrive at their ``arrival`` times (the loop sleeps
+        while nothing is active); otherwise all are queued at the start and
+        latencies count from the start."""
+        arrival = (lambda r: r.arrival) if realtime else (lambda r: 0.0)
+        pending = deque(sorted(requests, key=lambda r: (arrival(r), r.rid)))
+        t0 = time.perf_counter()
+        clock = lambda: time.perf_counter() - t0  # noqa: E731
+        self._arrival = arrival
+        results = []
+        while pending or self.queue or self.active:
+            now = clock()
+            while pending and arrival(pending[0]) <= now:
+                self.queue.append(pending.popleft())
+            act = self._launch() if self.active else None
+            n_before = len(self.active)
+            self._admit(now)
+            if len(self.active) > n_before:
+                self.main_stream.wait_stream(self.setup_stream)
+            if act:
+                results.extend(self._finish(act, clock))
+            elif not self.active and pending:
+                time.sleep(max(0.0, arrival(pending[0]) - clock()))
+        self.wall = clock()
+        return sorted(results, key=lambda r: r.rid)
+
+    def close(self):
+        for j in self.active:
+            j.eng.close()
+        for eng, _ in self.pool:
+            eng.close()
+        self.active = []
+        self.pool = []
+        self.used = 0
+        self.batch.close()
+
+
+def summarize(results, wall: float) -> dict:
+    """Throughput and latency percentiles of a served stream."""
+    lat = np.array([r.latency for r in results]) * 1e3
+    return {
+        "requests": len(results),
+        "solves_per_s": len(results) / wall if wall > 0 else None,
+        "wall_s": wall,
+        "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+        "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+        "mean_iterations": float(np.mean([r.niter for r in results])) if results else None,
+        "converged": int(sum(r.converged for r in results)),
+    }
+
+
+def run_stream(n_requests: int, rate: float, fp32_bound: float = 0.0, seed: int = 20261203,
+               memory_budget: int = None, denserms: float = 1e-6, device: int = 0, **stream_kw):
+    """Serve one seeded stream; returns (summary dict, results)."""
+    reqs = request_stream(n_requests, rate, seed=seed, **stream_kw)
+    srv = Server(device=device, memory_budget=memory_budget, fp32_bound=fp32_bound, denserms=denserms)
+    try:
+        res = srv.serve(reqs, realtime=True)
+        s = summarize(res, srv.wall)
+        for kind in ("molecule", "qmmm"):
+            sub = [r for r in res if r.kind == kind]
+            if sub:
+                lat = np.array([r.latency for r in sub]) * 1e3
+                s[kind] = {"requests": len(sub), "p50_ms": float(np.percentile(lat, 50)),
+                           "p99_ms": float(np.percentile(lat, 99)),
+                           "mean_iterations": float(np.mean([r.niter for r in sub]))}
+        s["host_seconds"] = {k: round(v, 3) for k, v in srv.timers.items()}
+        s.update({"rate_per_s": rate, "fp32_bound": fp32_bound, "memory_budget_bytes": srv.budget,
+                  "peak_bytes": srv.peak_used, "rejected": len(srv.rejected), "batch_steps": srv.steps,
+                  "mean_batch": float(np.mean(srv.batch_sizes)) if srv.batch_sizes else 0.0,
+                  "max_batch": int(max(srv.batch_sizes)) if srv.batch_sizes else 0,
+                  "warm_starts": int(sum(r.warm for r in res))})
+    finally:
+        srv.close()
+    return s, res
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="Serve a seeded stream of RHF requests on one GPU")
+    ap.add_argument("--requests", type=int, default=2048)
+    ap.add_argument("--rate", type=float, nargs="+", default=[50.0])
+    ap.add_argument("--fp32-bound", type=float, default=0.0)
+    ap.add_argument("--compare", action="store_true",
+                    help="serve each stream in plain FP64 and in the mixed form; report |dE| per request")
+    ap.add_argument("--budget-gb", type=float, default=None)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    budget = int(a.budget_gb * (1 << 30)) if a.budget_gb else None
+    report = []
+    for rate in a.rate:
+        if a.compare:
+            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget)
+            bound = a.fp32_bound if a.fp32_bound > 0 else 1e-5
+            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget)
+            e64 = {r.rid: r.E for r in r64}
+            dE = [abs(r.E - e64[r.rid]) for r in r32 if r.rid in e64]
+            s32["max_abs_dE_vs_fp64"] = float(max(dE)) if dE else None
+            line = {"rate_per_s": rate, "fp64": s64, "mixed": s32}
+        else:
+            line, _ = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget)
+        print(json.dumps(line), flush=True)
+        report.append(line)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(report, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -33,6 +33,22 @@ def test_oei_matches_oracle(bas):
         assert np.abs(x - y).max() <= 1e-10 * max(1.0, np.abs(y).max())
 
 
+def test_oei_many_point_charges_chunked_and_reproducible():
+    """Hundreds of point charges: the attraction is split over charge chunks and
+    summed in chunk order, so V matches the oracle and repeats bit for bit."""
+    _cuda()
+    from quick_b200.scf import oei
+    b = build_basis(water_cluster(3, 6.0), "6-31G*")
+    rng = np.random.default_rng(7)
+    ext = (rng.uniform(-25, 25, size=(900, 3)), np.where(np.arange(900) % 3 == 0, -0.834, 0.417))
+    S, T, V = oei(b, ext)
+    S0, T0, V0 = O.oei(b, ext)
+    assert np.abs(V - V0).max() <= 1e-10 * max(1.0, np.abs(V0).max())
+    assert np.abs(S - S0).max() <= 1e-12 and np.abs(T - T0).max() <= 1e-10 * np.abs(T0).max()
+    S2, T2, V2 = oei(b, ext)
+    assert V2.tobytes() == V.tobytes() and S2.tobytes() == S.tobytes()
+
+
 def test_rhf_energy_golden_h2o_631gs():
     _cuda()
     from quick_b200.scf import RHF

@@ -1,0 +1,151 @@
+"""GPU tests of the continuous-batching SCF server.
+
+The central property: a request's result served in a mix of other requests is
+the result it gets alone -- same energy, same iteration count, same density,
+bit for bit -- because the batched Fock build equals the one-molecule build bit
+for bit and every other step of a solve touches only its own matrices."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from quick_b200.basis import build_basis  # noqa: E402
+from quick_b200.molecules import water_cluster  # noqa: E402
+from quick_b200.serve import (Request, Server, cluster_box, request_bytes_estimate, request_stream,  # noqa: E402
+                              summarize)
+
+
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _mix():
+    reqs = []
+    for i, (nw, bas) in enumerate([(1, "STO-3G"), (3, "6-31G*"), (5, "STO-3G"), (2, "6-31G*"),
+                                   (8, "STO-3G"), (4, "6-31G*")]):
+        reqs.append(Request(i, water_cluster(nw, cluster_box(nw), seed=40 + i), bas))
+    # a QM/MM-style request: point charges, no series (cold start)
+    qm = [r for r in request_stream(40, 100.0, seed=2, qm_waters=3, n_charges=300, n_series=1)
+          if r.kind == "qmmm"][0]
+    reqs.append(Request(len(reqs), qm.mol, qm.basis, 0.0, qm.ext_charges, None, "qmmm"))
+    return reqs
+
+
+def test_alone_equals_in_mix():
+    _cuda()
+    reqs = _mix()
+    srv = Server(keep_densities=True)
+    mixed = srv.serve(reqs, realtime=False)
+    assert max(srv.batch_sizes) == len(reqs)        # all were in one batch at the start
+    srv.close()
+    for r in reqs:
+        s1 = Server(keep_densities=True)
+        alone = s1.serve([r], realtime=False)[0]
+        s1.close()
+        m = mixed[r.rid]
+        assert m.converged and alone.converged
+        assert m.niter == alone.niter, r.rid
+        assert m.E == alone.E, (r.rid, m.E, alone.E)
+        assert torch.equal(m.D, alone.D), r.rid
+
+
+def test_server_matches_rhf_run():
+    _cuda()
+    from quick_b200.scf import RHF
+    reqs = _mix()[:3]
+    srv = Server()
+    got = srv.serve(reqs, realtime=False)
+    srv.close()
+    for r, g in zip(reqs, got):
+        ref = RHF(build_basis(r.mol, r.basis), integral_cutoff=1e-10, ext_charges=r.ext_charges).run(denserms=1e-6)
+        assert g.niter == ref["niter"]
+        assert abs(g.E - ref["E"]) < 1e-10
+
+
+def test_memory_budget_admission():
+    _cuda()
+    reqs = _mix()
+    free = Server(pool=0)
+    alone = free.serve(reqs, realtime=False)
+    free.close()
+    measured = sum(r.bytes for r in alone)
+    est = max(request_bytes_estimate(build_basis(r.mol, r.basis)) for r in reqs)
+    # every request fits alone, all of them together do not
+    budget = max(est, measured // 2)
+    assert measured > budget
+    srv = Server(memory_budget=budget)
+    res = srv.serve(reqs, realtime=False)
+    assert len(res) == len(reqs) and all(r.converged for r in res)
+    assert max(srv.batch_sizes) < len(reqs)
+    assert not srv.active and srv.used == sum(b for _, b in srv.pool)
+    assert srv.peak_used <= srv.budget
+    for a, b in zip(alone, res):
+        assert a.E == b.E and a.niter == b.niter
+    srv.close()
+
+
+def test_estimate_bounds_measured_bytes():
+    _cuda()
+    from quick_b200.get2e import Get2e
+    from quick_b200.serve import context_bytes_estimate
+    for nw, bas in [(1, "STO-3G"), (6, "6-31G*"), (20, "6-31G*"), (40, "STO-3G")]:
+        b = build_basis(water_cluster(nw, cluster_box(nw), seed=nw), bas)
+        e = Get2e(b, integral_cutoff=1e-10, prim_limit=1e-11)
+        D = torch.zeros((b.nbasis, b.nbasis), dtype=torch.float64, device="cuda")
+        e.fock2e(D)
+        tot, items = e.device_bytes()
+        assert items < tot <= context_bytes_estimate(b), (nw, bas, tot, items, context_bytes_estimate(b))
+        e.close()
+
+
+def test_oversized_request_rejected():
+    _cuda()
+    reqs = _mix()[:2]
+    srv = Server(memory_budget=1 << 16)
+    res = srv.serve(reqs, realtime=False)
+    assert res == [] and len(srv.rejected) == 2
+    srv.close()
+
+
+def test_qmmm_warm_start_from_series():
+    _cuda()
+    reqs = [r for r in request_stream(60, 200.0, seed=8, qm_waters=4, n_charges=400, n_series=1)
+            if r.kind == "qmmm"][:3]
+    assert len(reqs) == 3
+    srv = Server(max_active=1)                      # one at a time: each repeat sees the last density
+    res = srv.serve(reqs, realtime=False)
+    srv.close()
+    assert [r.warm for r in res] == [False, True, True]
+    cold = Server()
+    c = cold.serve([Request(0, reqs[2].mol, reqs[2].basis, 0.0, reqs[2].ext_charges, None, "qmmm")],
+                   realtime=False)[0]
+    cold.close()
+    assert res[2].niter < c.niter
+    assert abs(res[2].E - c.E) < 1e-6
+
+
+def test_mixed_precision_server_within_1_microhartree():
+    _cuda()
+    reqs = _mix()
+    a = Server()
+    r64 = a.serve(reqs, realtime=False)
+    a.close()
+    b = Server(fp32_bound=1e-5)
+    r32 = b.serve(reqs, realtime=False)
+    b.close()
+    for x, y in zip(r64, r32):
+        assert abs(x.E - y.E) <= 1e-6, (x.rid, x.E, y.E)
+
+
+def test_realtime_stream_reports_latency():
+    _cuda()
+    reqs = request_stream(24, 200.0, seed=4, max_waters=6, qm_waters=4, n_charges=200, n_series=2)
+    srv = Server()
+    res = srv.serve(reqs, realtime=True)
+    s = summarize(res, srv.wall)
+    srv.close()
+    assert s["requests"] == 24 and s["converged"] == 24
+    assert 0 < s["p50_ms"] <= s["p99_ms"]
+    assert all(r.done >= r.arrival for r in res)
