@@ -198,6 +198,13 @@ int qk_class_profile(qk_ctx *ctx, int max_classes, int *cls, float *ms, long lon
 /* FP64 FMA throughput of device `device` measured by a short probe kernel (GFLOP/s). */
 int qk_fp64_peak(int device, double *gflops);
 
+/* Solve the n x n system A x = b (row-major device arrays, n <= 64) on `stream`
+ * with partial pivoting, in one warp; *ok_dev = 1, or 0 (and x = 0) when a pivot
+ * vanishes.  The DIIS step of an SCF iteration that stays on the device (no host
+ * synchronisation, so the iteration can be captured in a CUDA graph); QUICK
+ * solves the same system on the host (src/modules/quick_scf_module.f90:165-802). */
+int qk_small_solve(const double *A_dev, const double *b_dev, int n, double *x_dev, int *ok_dev, void *stream);
+
 /* One-electron integrals on device `device` (replaces the get1e path and the
  * reference's gpu_get_oei_, src/gpu/gpu_oei.cu:194; CPU twin
  * src/modules/quick_oei_module.f90:69-257).  Basis in QUICK's normalize_basis

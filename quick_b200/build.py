@@ -17,7 +17,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 
 
 def sources():
-    return [os.path.join(CSRC, "get2e.cu"), os.path.join(CSRC, "oei.cu")]
+    return [os.path.join(CSRC, "get2e.cu"), os.path.join(CSRC, "oei.cu"), os.path.join(CSRC, "scf.cu")]
 
 
 def _stale(target, deps):

@@ -1,0 +1,84 @@
+// Device helpers of the SCF iteration that must stay on the GPU stream (no host
+// synchronisation), so that a whole iteration can be captured as a CUDA graph.
+//
+// small_solve_kernel: the Pulay DIIS system (QUICK's electdiis,
+// src/modules/quick_scf_module.f90:165-802, which solves it on the host with
+// LAPACK) -- at most 64 unknowns -- by Gaussian elimination with partial
+// pivoting in one warp, the matrix held in shared memory.  A zero or non-finite
+// pivot sets *ok = 0 (the caller then keeps the plain Fock matrix).
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "quick_b200.h"
+
+namespace qk {
+
+constexpr int kSmallSolveMax = 64;
+
+__global__ void __launch_bounds__(32) small_solve_kernel(const double* __restrict__ A, const double* __restrict__ b,
+                                                         int n, double* __restrict__ x, int* __restrict__ ok) {
+    __shared__ double M[kSmallSolveMax][kSmallSolveMax + 1];
+    __shared__ int good;
+    const int lane = threadIdx.x;
+    for (int i = 0; i < n; ++i) {
+        for (int j = lane; j < n; j += 32) M[i][j] = A[(size_t)i * n + j];
+        if (lane == 0) M[i][n] = b[i];
+    }
+    if (lane == 0) good = 1;
+    __syncwarp();
+    for (int k = 0; k < n; ++k) {
+        // pivot: largest |M[i][k]|, i >= k (lowest index on ties)
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + lane; i < n; i += 32) {
+            const double v = fabs(M[i][k]);
+            if (v > best) { best = v; bi = i; }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (!(best > 0.0) || !isfinite(best)) {
+            if (lane == 0) good = 0;
+            break;
+        }
+        if (bi != k)
+            for (int j = lane; j <= n; j += 32) {
+                const double t = M[k][j];
+                M[k][j] = M[bi][j];
+                M[bi][j] = t;
+            }
+        __syncwarp();
+        const double piv = M[k][k];
+        for (int i = k + 1; i < n; ++i) {
+            const double f = M[i][k] / piv;
+            __syncwarp();
+            for (int j = k + lane; j <= n; j += 32) M[i][j] -= f * M[k][j];
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        if (good) {
+            for (int i = n - 1; i >= 0; --i) {
+                double s = M[i][n];
+                for (int j = i + 1; j < n; ++j) s -= M[i][j] * x[j];
+                x[i] = s / M[i][i];
+                if (!isfinite(x[i])) good = 0;
+            }
+        }
+        if (!good)
+            for (int i = 0; i < n; ++i) x[i] = 0.0;
+        *ok = good;
+    }
+}
+
+}  // namespace qk
+
+extern "C" int qk_small_solve(const double* A, const double* b, int n, double* x, int* ok, void* stream) {
+    if (!A || !b || !x || !ok || n < 1 || n > qk::kSmallSolveMax) return QK_ERR_INVALID_ARG;
+    qk::small_solve_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(A, b, n, x, ok);
+    return cudaGetLastError() == cudaSuccess ? QK_OK : QK_ERR_CUDA;
+}

@@ -212,3 +212,183 @@ class SCFState:
         r = self.rhf
         return {"E": self.Eel + r.Ecore, "Eel": self.Eel, "Ecore": r.Ecore, "D": self.D, "F": self.F,
                 "niter": self.it, "converged": self.converged, "history": self.history}
+
+
+def gershgorin_range(Fo) -> float:
+    """Width of the Gershgorin interval of a symmetric matrix (the interval the
+    SP2 projection maps onto [0, 1])."""
+    import torch
+    d = torch.diagonal(Fo)
+    rad = torch.abs(Fo).sum(dim=1) - torch.abs(d)
+    return float(torch.max(d + rad) - torch.min(d - rad))
+
+
+def sp2_steps(eigvals, nocc: int, width: float = None) -> int:
+    """SP2 projection steps for a spectrum ``eigvals`` (ascending) with ``nocc``
+    occupied levels mapped from an interval of ``width`` (default: the spectral
+    range): twice log2(2 width / HOMO-LUMO gap) -- the steps that open the gap --
+    plus 28 for the quadratic end game (which takes 15-22 steps to reach 1e-12 on
+    spectra of 60-600 levels), clamped to [30, 160]."""
+    e = [float(x) for x in eigvals]
+    gap = max(e[nocc] - e[nocc - 1], 1e-6) if 0 < nocc < len(e) else 1.0
+    w = max(width if width is not None else e[-1] - e[0], 2.0 * gap)
+    return int(min(160, max(30, math.ceil(2.0 * math.log2(2.0 * w / gap)) + 28)))
+
+
+class GraphSCF:
+    """RHF whose whole iteration -- Fock build, energy, Pulay DIIS and the new
+    density -- is one CUDA graph, replayed once per cycle.
+
+    What keeps the iteration free of host synchronisation:
+
+    * the Fock build accumulates ``base + G(D - Dref)`` into a static matrix:
+      ``base = H, Dref = 0`` for the full builds of the first cycles, and
+      ``base = F_prev, Dref = D_prev`` afterwards (QUICK's incremental build,
+      ``quick_scf_operator_module.f90:69-82``);
+    * the DIIS history is a fixed set of ``maxdiis`` slots shifted each cycle,
+      with the unused slots masked out of the B matrix by a device-side count,
+      and the DIIS system is solved by ``qk_small_solve`` (partial pivoting in
+      one warp; a vanishing pivot keeps the plain Fock matrix, as in
+      :class:`SCFState`);
+    * the density is the projector onto the ``nocc`` lowest levels of X^T F X by
+      SP2 purification (Niklasson, Phys. Rev. B 66, 155115 (2002)): Y0 maps the
+      Gershgorin interval onto [1, 0], then Y <- Y^2 or 2Y - Y^2, whichever trace
+      is nearer nocc, a fixed number of steps (:func:`sp2_steps`, from the
+      spectrum of the guess).  The projector is the same one diagonalisation
+      gives; D = 2 X Y X^T.
+
+    Each replay also writes (Eel, PRMS, PCHANGE) of the cycle; the host reads
+    those three numbers for QUICK's convergence test.  ``graph=False`` runs the
+    same body eagerly (same kernels, same numbers).
+    """
+
+    def __init__(self, rhf, maxdiis: int = 10, sp2: int = None):
+        torch = rhf.torch
+        self.rhf, self.torch = rhf, torch
+        n, m, k = rhf.basis.nbasis, rhf.X.shape[1], maxdiis
+        dev, dt = rhf.device, torch.float64
+        z = lambda *s: torch.zeros(s, dtype=dt, device=dev)  # noqa: E731
+        self.k, self.m = k, m
+        self.D, self.Dref, self.base, self.F = z(n, n), z(n, n), z(n, n), z(n, n)
+        self.errs, self.focks = z(k, m, m), z(k, n, n)
+        self.valid = torch.zeros((), dtype=torch.int64, device=dev)
+        self.idx = torch.arange(k, device=dev)
+        self.B, self.rhs, self.c = z(k + 1, k + 1), z(k + 1), z(k + 1)
+        self.rhs[k] = -1.0
+        self.ok = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.eye_k = torch.eye(k, dtype=dt, device=dev)
+        self.eye_m = torch.eye(m, dtype=dt, device=dev)
+        self.out = z(4)
+        self.zero = torch.zeros((), dtype=dt, device=dev)
+        self.minus_one = torch.full((), -1.0, dtype=dt, device=dev)
+        self.recaptures = 0
+        self.sp2 = sp2
+        self.graph = None
+
+    def _density(self, Fd):
+        torch = self.torch
+        X = self.rhf.X
+        Fo = X.T @ Fd @ X
+        d = torch.diagonal(Fo)
+        rad = torch.abs(Fo).sum(dim=1) - torch.abs(d)
+        emin, emax = torch.min(d - rad), torch.max(d + rad)
+        Y = (emax * self.eye_m - Fo) / (emax - emin)
+        ne = float(self.rhf.nocc)
+        for _ in range(self.sp2):
+            Y2 = Y @ Y
+            t0, t1 = torch.trace(Y), torch.trace(Y2)
+            Y = torch.where(torch.abs(t1 - ne) < torch.abs(2.0 * t0 - t1 - ne), Y2, 2.0 * Y - Y2)
+        # idempotency defect tr(Y - Y^2): zero once the projection has converged
+        self.out[3].copy_(torch.trace(Y) - torch.sum(Y * Y))
+        return 2.0 * (X @ Y @ X.T)
+
+    def _body(self):
+        torch = self.torch
+        r, k = self.rhf, self.k
+        stream = torch.cuda.current_stream(r.device)
+        self.F.copy_(self.base)
+        r.eng.fock2e(self.D - self.Dref, o=self.F, stream=stream)
+        F, D = self.F, self.D
+        Eel = 0.5 * torch.sum(D * (r.H + F))
+        e = r.X.T @ (F @ D @ r.S - r.S @ D @ F) @ r.X
+        self.errs.copy_(torch.roll(self.errs, -1, 0))
+        self.errs[k - 1].copy_(e)
+        self.focks.copy_(torch.roll(self.focks, -1, 0))
+        self.focks[k - 1].copy_(F)
+        self.valid.copy_(torch.clamp(self.valid + 1, max=k))
+        live = self.idx >= (k - self.valid)
+        E = self.errs.reshape(k, -1)
+        self.B[:k, :k].copy_(torch.where(live[:, None] & live[None, :], E @ E.T, self.eye_k))
+        side = torch.where(live, self.minus_one, self.zero)
+        self.B[:k, k].copy_(side)
+        self.B[k, :k].copy_(side)
+        self.B[k, k].zero_()
+        check(lib().qk_small_solve(ctypes.c_void_p(self.B.data_ptr()), ctypes.c_void_p(self.rhs.data_ptr()), k + 1,
+                                   ctypes.c_void_p(self.c.data_ptr()), ctypes.c_void_p(self.ok.data_ptr()),
+                                   ctypes.c_void_p(stream.cuda_stream)), "qk_small_solve")
+        Fd = torch.einsum("k,kij->ij", self.c[:k], self.focks)
+        Fd = torch.where((self.ok[0] == 1) & torch.isfinite(Fd).all(), Fd, F)
+        Dn = self._density(Fd)
+        dd = Dn - D
+        self.out[0].copy_(Eel)
+        self.out[1].copy_(torch.sqrt(torch.mean(dd * dd)))
+        self.out[2].copy_(torch.abs(dd).max())
+        self.Dref.copy_(D)
+        self.base.copy_(F)
+        self.D.copy_(Dn)
+
+    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess: str = "gwh", ncyc: int = 3, D0=None,
+            graph: bool = True):
+        torch = self.torch
+        r = self.rhf
+        t0 = time.perf_counter()
+        if guess == "core":
+            Fg = r.H
+        else:
+            dg = torch.diagonal(r.H)
+            Fg = 0.875 * r.S * (dg[:, None] + dg[None, :])
+            Fg.fill_diagonal_(0.0)
+            Fg += torch.diag(dg)
+        Fo = r.X.T @ Fg @ r.X
+        e, C = torch.linalg.eigh(Fo)
+        if self.sp2 is None:
+            self.sp2 = sp2_steps(e.cpu().numpy(), r.nocc, gershgorin_range(Fo))
+        if D0 is not None:
+            self.D.copy_(D0)
+        else:
+            Co = r.X @ C[:, : r.nocc]
+            self.D.copy_(2.0 * Co @ Co.T)
+        self.valid.zero_()
+        self.errs.zero_()
+        self.focks.zero_()
+        history = []
+        converged = False
+        for it in range(1, maxiter + 1):
+            if it < ncyc:
+                self.base.copy_(r.H)
+                self.Dref.zero_()
+            if graph and it >= ncyc:
+                if self.graph is None:
+                    torch.cuda.synchronize(r.device)
+                    self.graph = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(self.graph):
+                        self._body()
+                self.graph.replay()
+            else:
+                self._body()
+            Eel, prms, pchange, defect = (float(x) for x in self.out.cpu().numpy())
+            r.fock_builds += 1
+            if abs(defect) > 1e-9 * max(1, r.nocc) and self.sp2 < 200:
+                # the projection needs more steps for this spectrum: recapture with more
+                self.sp2 += 16
+                self.graph = None
+                self.recaptures += 1
+            history.append((it, Eel + r.Ecore, prms))
+            if it >= 3 and prms < denserms and pchange < 100 * denserms:
+                converged = True
+                break
+        torch.cuda.synchronize(r.device)
+        D = self.Dref.clone() if converged else self.D.clone()
+        return {"E": Eel + r.Ecore, "Eel": Eel, "Ecore": r.Ecore, "D": D, "F": self.F.clone(), "niter": it,
+                "converged": converged, "history": history, "seconds": time.perf_counter() - t0,
+                "sp2_steps": self.sp2, "graph": self.graph is not None, "recaptures": self.recaptures}
