@@ -87,7 +87,8 @@ void gpu_delete_(int *ierr);
 /* ======================================================= context API */
 typedef struct qk_ctx qk_ctx;
 
-/* Status of the most recent failing call on the default (drop-in) context. */
+/* Status of the most recent failing call (QK_OK if none since gpu_new_, which
+ * starts a drop-in session). */
 int qk_last_status(void);
 const char *qk_status_string(int status);
 /* Rows of gccoeff/gcexpo expected by gpu_upload_basis_ (reference MAXPRIM; default 20). */
@@ -183,6 +184,21 @@ int qk_batch_fock2e(qk_batch *batch, int n, qk_ctx *const *ctx, const double *co
 int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int *launches);
 /* Kernel launches of one build (for launch accounting). */
 int qk_launches_per_build(qk_ctx *ctx);
+
+/* Launch shape of a build: the class kernels run concurrently over `nstreams`
+ * auxiliary streams forked from the caller's stream (1..4, default 4), or one after
+ * another on the caller's stream (0).  A tuning knob: which is faster depends on
+ * the molecule's mix of classes. */
+int qk_set_streams(qk_ctx *ctx, int nstreams);
+
+/* Launch shape of one integral class (index as listed by qk_class_profile):
+ * warps per block (1..max, 0 = default: 4 for the per-lane classes, the
+ * shared-memory fit for the cooperative ones) and a cap on resident blocks per SM
+ * (0 = as many as fit).  The grid stays persistent (blocks loop over the class's
+ * work items), so any shape computes the same result.  qk_class_launch reads the
+ * shape in force, the largest allowed warps per block and the current grid. */
+int qk_set_class_launch(qk_ctx *ctx, int cls, int warps_per_block, int blocks_per_sm);
+int qk_class_launch(qk_ctx *ctx, int cls, int *warps_per_block, int *max_warps, int *blocks_per_sm, int *grid);
 
 /* Per-class measurement: `events` records CUDA events around every class launch on the
  * launching stream; `stats` counts the quartets and primitive quartets each class

@@ -82,6 +82,74 @@ __device__ __forceinline__ void boys_scaled(double T, double scale, const double
 
 // Boys table F_m(k * dT), m < kBoysNM, from the convergent series
 // F_m(T) = exp(-T) sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)) in long double.
+// F_0..F_M at T from a per-M row table (kBoysNT rows of 8 doubles: F_M..F_{M+6}
+// at T_k, then exp(-T_k)): the same arithmetic as boys_scaled, with four 16-byte
+// loads of one 64-byte row per evaluation instead of eight 8-byte ones.
+constexpr int kBoysRow = 8;
+template <int M>
+__device__ __forceinline__ void boys_scaled_rows(double T, double scale, const double2* __restrict__ rows,
+                                                 double* F) {
+    if (T < kBoysTmax) {
+        const int k = __double2int_rn(T * kBoysInvDT);
+        const double u = k * kBoysDT - T;
+        const double2* r = rows + k * (kBoysRow / 2);
+        const double2 c01 = __ldg(r), c23 = __ldg(r + 1), c45 = __ldg(r + 2), c6e = __ldg(r + 3);
+        double f = c6e.x * (1.0 / 720.0);
+        f = fma(f, u, c45.y * (1.0 / 120.0));
+        f = fma(f, u, c45.x * (1.0 / 24.0));
+        f = fma(f, u, c23.y * (1.0 / 6.0));
+        f = fma(f, u, c23.x * 0.5);
+        f = fma(f, u, c01.y);
+        f = fma(f, u, c01.x);
+        if (M == 0) {
+            F[0] = f * scale;
+        } else {
+            double eu = fma(u, 1.0 / 720.0, 1.0 / 120.0);
+            eu = fma(eu, u, 1.0 / 24.0);
+            eu = fma(eu, u, 1.0 / 6.0);
+            eu = fma(eu, u, 0.5);
+            eu = fma(eu, u, 1.0);
+            eu = fma(eu, u, 1.0);
+            const double e = c6e.y * eu;
+            const double T2 = 2.0 * T;
+            double fm = f;
+            F[M] = fm * scale;
+#pragma unroll
+            for (int m = M; m > 0; --m) {
+                fm = fma(T2, fm, e) * (1.0 / (2 * m - 1));
+                F[m - 1] = fm * scale;
+            }
+        }
+    } else {
+        double f0 = kHalfSqrtPi * rsqrt(T);
+        F[0] = f0 * scale;
+        if (M > 0) {
+            const double e = exp(-T);
+            const double h = 0.5 / T;
+            double fm = f0;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                fm = fma((double)(2 * m + 1), fm, -e) * h;
+                F[m + 1] = fm * scale;
+            }
+        }
+    }
+}
+
+// Row tables for M = 0 .. 4 kMaxL from boys_table(): block M holds kBoysNT rows
+// of kBoysRow doubles (F_M..F_{M+6}, exp(-T_k)).
+inline std::vector<double> boys_row_tables(const std::vector<double>& tab) {
+    const int nM = 4 * kMaxL + 1;
+    std::vector<double> r((size_t)nM * kBoysNT * kBoysRow);
+    for (int M = 0; M < nM; ++M)
+        for (int k = 0; k < kBoysNT; ++k) {
+            double* row = &r[((size_t)M * kBoysNT + k) * kBoysRow];
+            for (int j = 0; j < 7; ++j) row[j] = tab[(size_t)k * kBoysNM + M + j];
+            row[7] = tab[(size_t)kBoysNT * kBoysNM + k];
+        }
+    return r;
+}
+
 inline std::vector<double> boys_table() {
     std::vector<double> t((size_t)kBoysNT * kBoysNM);
     for (int k = 0; k < kBoysNT; ++k) {

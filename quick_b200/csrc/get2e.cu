@@ -66,6 +66,7 @@ struct DevData {
     const double* __restrict__ pp_PAy;
     const double* __restrict__ pp_PAz;
     const double* __restrict__ boys;     // kBoysNT x kBoysNM
+    const double2* __restrict__ boys8;   // row tables, M = 0..4 kMaxL (boys_row_tables)
     const double* __restrict__ D;        // nbasis^2
     const double* __restrict__ cutmat;   // nshell^2
     unsigned long long* __restrict__ A;  // nbasis^2 fixed point
@@ -90,8 +91,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // small-bound quartets of the mixed form.  Geometry and the Boys function are
 // always evaluated in FP64 and rounded to R afterwards.
 template <int La, int Lb, int Lc, int Ld, typename R = double>
-__device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int bnp, int bps, int kp0, int knp,
-                                                 int kps,
+__device__ __forceinline__ void contract_quartet(const DevData& d, const double2* __restrict__ bt, int bp0, int bnp,
+                                                 int bps, int kp0, int knp, int kps,
                                                  const double C[3], double dnmax, bool prim_screen,
                                                  R* acc, int* nprim_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
@@ -121,7 +122,7 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const double pref = Kab * __ldg(d.pp_K + pj) * rs;
             double F[M + 1];
-            boys_scaled<M>(T, pref, d.boys, F);
+            boys_scaled_rows<M>(T, pref, bt, F);
             VrrGeom<R> G;
             G.PA[0] = R(PAx); G.PA[1] = R(PAy); G.PA[2] = R(PAz);
             G.WP[0] = R(-rho_z * PQx); G.WP[1] = R(-rho_z * PQy); G.WP[2] = R(-rho_z * PQz);
@@ -144,8 +145,8 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, int bp0, int 
 // Lane-private updates go straight to A; the bra J block is returned in jab
 // (already weighted) for the warp reduction.
 template <int La, int Lb, int Lc, int Ld>
-__device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, bool fp32, double* jab_out,
-                                             int* nq_done, int* np_done) {
+__device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __restrict__ bt, int P, int Q, bool fp32,
+                                             double* jab_out, int* nq_done, int* np_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND;
     constexpr int NE = Cls::NE, NF = Cls::NF, NAB = NA * NB;
@@ -170,12 +171,12 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, int P, int Q, boo
     if (fp32) {
         // mixed form: small-bound quartet, vertical recursion and contraction in FP32
         float accf[NE * NF];
-        contract_quartet<La, Lb, Lc, Ld, float>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q],
+        contract_quartet<La, Lb, Lc, Ld, float>(d, bt, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q],
                                                 d.pr_npp[Q], d.pr_pps[Q], Cc, dnmax, true, accf, np_done);
 #pragma unroll
         for (int i = 0; i < NE * NF; ++i) acc[i] = (double)accf[i];
     } else {
-        contract_quartet<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q],
+        contract_quartet<La, Lb, Lc, Ld>(d, bt, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q],
                                          d.pr_pps[Q], Cc, dnmax, true, acc, np_done);
     }
 
@@ -505,14 +506,29 @@ fock_coop_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __
     }
 }
 
+// The class's Boys row table (kBoysNT rows of 64 bytes): an evaluation reads one
+// row with four 16-byte loads, served from L1 for the hot part of the T range.
+// (Staging the 46 KB table in shared memory costs more in occupancy than it
+// saves in load latency: measured 1.8x slower on the ssss class.)
+template <int M>
+__device__ __forceinline__ const double2* class_boys_rows(const double2* __restrict__ src) {
+    return src + (size_t)M * kBoysNT * (kBoysRow / 2);
+}
+
+// Per-lane class kernels launch with 1..kMaxLaneWarps warps per block (default
+// kWarpsPerBlock; the autotuner picks per class).  The bound leaves the register
+// allocation as it is for 128-thread blocks (255 registers allowed either way).
+constexpr int kMaxLaneWarps = 8;
+
 // Work item: x = bra pair, y = first ket pair, z = number of kets (<= 32),
 // w = 1 for the mixed form's FP32 quartets.
 template <int La, int Lb, int Lc, int Ld>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+__global__ void __launch_bounds__(32 * kMaxLaneWarps)
 fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NAB = Cls::NA * Cls::NB;
     const int lane = threadIdx.x & 31;
+    const double2* bt = class_boys_rows<Cls::M>(d.boys8);
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(counter, 1);
@@ -523,7 +539,7 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, bt, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
         if (d.stats) {
             const unsigned sq = __reduce_add_sync(0xffffffffu, (unsigned)nq);
             const unsigned sp = __reduce_add_sync(0xffffffffu, (unsigned)np);
@@ -568,12 +584,13 @@ __device__ __forceinline__ int batch_find_seg(const BatchSeg* __restrict__ segs,
 }
 
 template <int La, int Lb, int Lc, int Ld>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+__global__ void __launch_bounds__(32 * kMaxLaneWarps)
 fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restrict__ segs, int nseg, int n_items,
                         int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NAB = Cls::NA * Cls::NB;
     const int lane = threadIdx.x & 31;
+    const double2* bt = class_boys_rows<Cls::M>(dl[0].boys8);
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(counter, 1);
@@ -586,7 +603,7 @@ fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restri
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, bt, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
         const int P = w.x;
         const int fa = d.q_f0[d.pr_qa[P]], fb = d.q_f0[d.pr_qb[P]];
 #pragma unroll
@@ -687,7 +704,8 @@ schwarz_kernel(DevData d, const int2* __restrict__ work, int n_work, const int* 
     if (mode >= 0) { p0 += mode * ps; np = 1; }
     double acc[NE * NF];
     int ndone = 0;
-    contract_quartet<La, Lb, La, Lb>(d, p0, np, ps, p0, np, ps, Cc, 0.0, false, acc, &ndone);
+    contract_quartet<La, Lb, La, Lb>(d, d.boys8 + (size_t)Cls::M * kBoysNT * (kBoysRow / 2), p0, np, ps, p0, np, ps,
+                                     Cc, 0.0, false, acc, &ndone);
     double t1[NF * NAB];
 #pragma unroll
     for (int f = 0; f < NF; ++f) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, AB[0], AB[1], AB[2]);
@@ -901,7 +919,7 @@ void launch_fock(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData& dd
     if constexpr (EriClass<a, b, c, e>::COOP)
         fock_coop_kernel<a, b, c, e><<<g, bl, smem, s>>>(dd, it, n, cnt);
     else
-        fock_class_kernel<a, b, c, e><<<g, bl, 0, s>>>(dd, it, n, cnt);
+        fock_class_kernel<a, b, c, e><<<g, bl, smem, s>>>(dd, it, n, cnt);
 }
 template <int a, int b, int c, int e>
 const void* fock_fn_ptr() {
@@ -917,7 +935,7 @@ void launch_fock_batch(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevDa
     if constexpr (EriClass<a, b, c, e>::COOP)
         fock_coop_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
     else
-        fock_class_kernel_batch<a, b, c, e><<<g, bl, 0, s>>>(dl, segs, nseg, n, cnt);
+        fock_class_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
 }
 template <int a, int b, int c, int e>
 const void* fock_batch_fn_ptr() {
@@ -964,6 +982,8 @@ struct ClassWork {
     std::vector<int4> items;
     DevBuf<int4> d_items;
     long long nquart = 0, nprimq = 0, nquart32 = 0;
+    int block = 0;        // threads per block of the class launch
+    size_t smem = 0;      // dynamic shared memory of a block
     int grid = 0;
 };
 
@@ -982,6 +1002,9 @@ struct qk_ctx {
     std::vector<double> Ycut, cutprim;   // nshell^2, jbasis^2 (symmetric)
     double integralCutoff = 1e-7, primLimit = 1e-8;
     double fp32_bound = 0.0;          // mixed form: FP32 below this Schwarz bound product
+    int nstreams = 4;                 // class kernels run over this many streams (0: one after another)
+    int cls_wpb[qk::kNumClasses] = {};    // warps per block of each class launch (0: default)
+    int cls_bpsm[qk::kNumClasses] = {};   // cap on resident blocks per SM (0: as many as fit)
     unsigned long long work_version = 0;   // bumped whenever the work lists are rebuilt
     double built_fp32 = -1.0;
     double built_cut = -1.0;
@@ -992,7 +1015,7 @@ struct qk_ctx {
     long long last_quart = 0, last_primq = 0;
     int num_sms = 148;
     // device buffers
-    qk::DevBuf<double> d_xyz, d_boys, d_D, d_cutmat, d_o;
+    qk::DevBuf<double> d_xyz, d_boys, d_boys8, d_D, d_cutmat, d_o;
     qk::DevBuf<int> d_q_atom, d_q_f0, d_q_parent, d_q_prim0, d_q_nprim, d_shell_f0, d_shell_f1;
     qk::DevBuf<unsigned long long> d_A;
     qk::DevBuf<int> d_counters;
@@ -1093,6 +1116,7 @@ static DevData make_devdata(qk_ctx* c) {
     d.pp_PAy = c->pairs.d_PAy.p;
     d.pp_PAz = c->pairs.d_PAz.p;
     d.boys = c->d_boys.p;
+    d.boys8 = (const double2*)c->d_boys8.p;
     d.cut = c->integralCutoff;
     d.primLimit = c->primLimit;
     return d;
@@ -1213,6 +1237,28 @@ static int upload_pairs(qk_ctx* c) {
 
 // Work items of every class: (bra pair, first ket, count) chunks of <= 32
 // kets that pass the Schwarz test, unique quartets only.
+// Launch shape of class ci for the context's current work list: warps per block
+// (tuned or default), the matching dynamic shared memory (cooperative classes:
+// one work area per warp), and a persistent grid of as many blocks as can be
+// resident (optionally capped per SM), but no more than there are items.
+static int class_launch_shape(qk_ctx* c, int ci) {
+    const ClassEntry& ce = g_classes[ci];
+    ClassWork& W = c->work[ci];
+    const int wpb = c->cls_wpb[ci] > 0 ? c->cls_wpb[ci] : (ce.coop ? ce.coop_warps : kWarpsPerBlock);
+    const size_t smem = ce.coop ? ce.smem / ce.coop_warps * wpb : 0;
+    if (smem > 48 * 1024)
+        QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
+    int bps = 0;
+    QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(), 32 * wpb, smem));
+    if (bps < 1) return fail(QK_ERR_CUDA, "class kernel cannot be resident");
+    if (c->cls_bpsm[ci] > 0) bps = std::min(bps, c->cls_bpsm[ci]);
+    const long long need = ((long long)W.items.size() + wpb - 1) / wpb;
+    W.grid = (int)std::max<long long>(1, std::min<long long>((long long)bps * c->num_sms, need));
+    W.block = 32 * wpb;
+    W.smem = smem;
+    return QK_OK;
+}
+
 static int build_work(qk_ctx* c) {
     PairTable& T = c->pairs;
     const double cut = c->integralCutoff;
@@ -1274,14 +1320,8 @@ static int build_work(qk_ctx* c) {
         for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
         QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
         if (!W.items.empty()) {
-            const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
-            if (ce.smem > 48 * 1024)
-                QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
-            int bps = 0;
-            QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(), 32 * wpb, ce.smem));
-            if (bps < 1) return fail(QK_ERR_CUDA, "class kernel cannot be resident");
-            const long long need = ((long long)W.items.size() + wpb - 1) / wpb;
-            W.grid = (int)std::min<long long>((long long)bps * c->num_sms, need);
+            int st = class_launch_shape(c, ci);
+            if (st) return st;
             c->launches++;
         }
     }
@@ -1353,7 +1393,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     // angular momentum, latency-bound classes first so the bulk classes fill the
     // remaining SMs).  With per-class event timing on they run one after another
     // on `s`, so that every class kernel is timed alone.
-    const bool concurrent = !c->profile_events;
+    const bool concurrent = !c->profile_events && c->nstreams > 0;
     if (concurrent) QK_CUDA_TRY(cudaEventRecord(c->fork_ev, s));
     bool used[qk_ctx::kAux] = {};
     int slot = 0;
@@ -1361,7 +1401,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         ClassWork& W = c->work[ci];
         cudaStream_t ls = s;
         if (concurrent) {
-            const int k = slot++ % qk_ctx::kAux;
+            const int k = slot++ % c->nstreams;
             ls = c->aux[k];
             if (!used[k]) {
                 QK_CUDA_TRY(cudaStreamWaitEvent(ls, c->fork_ev, 0));
@@ -1371,7 +1411,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         if (c->profile_stats) d.stats = c->d_stats.p + 2 * ci;
         if (c->profile_events) QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci], ls));
         const ClassEntry& ce = g_classes[ci];
-        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? ce.coop_warps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
+        ce.fn(dim3(W.grid), dim3(W.block), W.smem, ls, d, W.d_items.p,
               (int)W.items.size(), c->d_counters.p + ci);
         QK_CUDA_TRY(cudaGetLastError());
         if (c->profile_events) {
@@ -1483,7 +1523,7 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
             used[k] = true;
         }
         const ClassEntry& ce = g_classes[ci];
-        ce.fn(dim3(W.grid), dim3(32 * (ce.coop ? ce.coop_warps : kWarpsPerBlock)), ce.smem, ls, d, W.d_items.p,
+        ce.fn(dim3(W.grid), dim3(W.block), W.smem, ls, d, W.d_items.p,
               (int)W.items.size(), counters + ci);
         QK_CUDA_TRY(cudaGetLastError());
     }
@@ -1579,8 +1619,15 @@ qk_ctx* qk_create(int device, int* status) {
         if (status) *status = fail(QK_ERR_CUDA, "stream creation failed");
         return nullptr;
     }
-    std::vector<double> tab = boys_table();
-    if (c->d_boys.upload(tab, c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    // the tables are the same for every context: computed once per process
+    static std::once_flag once;
+    static std::vector<double> tab, rows;
+    std::call_once(once, [] {
+        tab = boys_table();
+        rows = boys_row_tables(tab);
+    });
+    if (c->d_boys.upload(tab, c->stream) != cudaSuccess || c->d_boys8.upload(rows, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
         cudaStreamDestroy(c->stream);
         delete c;
         if (status) *status = fail(QK_ERR_CUDA, "Boys table upload failed");
@@ -2058,7 +2105,7 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
                      T.d_Y.bytes(), T.d_zeta.bytes(), T.d_oo2z.bytes(), T.d_K.bytes(), T.d_cut.bytes(),
                      T.d_Px.bytes(), T.d_Py.bytes(), T.d_Pz.bytes(), T.d_PAx.bytes(), T.d_PAy.bytes(),
-                     T.d_PAz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
+                     T.d_PAz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
                      c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(),
                      c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
                      c->d_A.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
@@ -2077,6 +2124,41 @@ int qk_last_work(qk_ctx* c, long long* quartets, long long* primq, int* launches
 }
 
 int qk_launches_per_build(qk_ctx* c) { return c ? c->launches : 0; }
+
+int qk_set_class_launch(qk_ctx* c, int ci, int warps_per_block, int blocks_per_sm) {
+    if (!c || ci < 0 || ci >= kNumClasses) return fail(QK_ERR_INVALID_ARG, "qk_set_class_launch: class index");
+    const ClassEntry& ce = g_classes[ci];
+    const int maxw = ce.coop ? ce.coop_warps : kMaxLaneWarps;
+    if (warps_per_block < 0 || warps_per_block > maxw || blocks_per_sm < 0 || blocks_per_sm > 64)
+        return fail(QK_ERR_INVALID_ARG, "qk_set_class_launch: warps per block or blocks per SM out of range");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    c->cls_wpb[ci] = warps_per_block;
+    c->cls_bpsm[ci] = blocks_per_sm;
+    if (!c->work[ci].items.empty()) return class_launch_shape(c, ci);
+    return QK_OK;
+}
+
+int qk_class_launch(qk_ctx* c, int ci, int* warps_per_block, int* max_warps, int* blocks_per_sm, int* grid) {
+    if (!c || ci < 0 || ci >= kNumClasses) return fail(QK_ERR_INVALID_ARG, "qk_class_launch: class index");
+    const ClassEntry& ce = g_classes[ci];
+    std::lock_guard<std::mutex> g(c->mu);
+    const ClassWork& W = c->work[ci];
+    if (warps_per_block)
+        *warps_per_block = W.block > 0 ? W.block / 32
+                                       : (c->cls_wpb[ci] > 0 ? c->cls_wpb[ci] : (ce.coop ? ce.coop_warps : kWarpsPerBlock));
+    if (max_warps) *max_warps = ce.coop ? ce.coop_warps : kMaxLaneWarps;
+    if (blocks_per_sm) *blocks_per_sm = c->cls_bpsm[ci];
+    if (grid) *grid = W.items.empty() ? 0 : W.grid;
+    return QK_OK;
+}
+
+int qk_set_streams(qk_ctx* c, int nstreams) {
+    if (!c || nstreams < 0 || nstreams > qk_ctx::kAux) return fail(QK_ERR_INVALID_ARG, "qk_set_streams: 0..4");
+    std::lock_guard<std::mutex> g(c->mu);
+    c->nstreams = nstreams;
+    return QK_OK;
+}
 
 int qk_set_profiling(qk_ctx* c, int events, int stats) {
     if (!c) return fail(QK_ERR_INVALID_ARG, "null context");
@@ -2154,6 +2236,7 @@ int qk_fp64_peak(int device, double* gflops) {
 
 // ------------------------------------------------------------- drop-in layer
 void gpu_new_(int* ierr) {
+    g_last_status = QK_OK;   // a new drop-in session reports only its own failures
     qk_ctx* c = qk_default_ctx();
     if (ierr) *ierr = c ? 0 : QK_ERR_NO_DEVICE;
 }

@@ -152,6 +152,10 @@ class Get2e:
         check(lib().qk_fock2e_host(self.h, _p(D), cm, _p(out)), "qk_fock2e_host")
         return out
 
+    def set_streams(self, nstreams: int):
+        """Class kernels over ``nstreams`` concurrent streams (0: one after another)."""
+        check(lib().qk_set_streams(self.h, int(nstreams)), "qk_set_streams")
+
     def prepare(self):
         """Build the pair tables and work lists now rather than in the first build."""
         check(lib().qk_prepare(self.h), "qk_prepare")
