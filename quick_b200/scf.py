@@ -150,6 +150,7 @@ class SCFState:
         self.torch = rhf.torch
         self.denserms, self.maxiter = denserms, maxiter
         self.incremental, self.ncyc, self.maxdiis = incremental, ncyc, maxdiis
+        self.warm = D0 is not None
         self.D = D0.clone() if D0 is not None else rhf.guess(guess)
         self.errs, self.focks = [], []
         self.F = self.F_prev = self.D_prev = self.Dn = None
@@ -302,12 +303,11 @@ class GraphSCF:
         self.out[3].copy_(torch.trace(Y) - torch.sum(Y * Y))
         return 2.0 * (X @ Y @ X.T)
 
-    def _body(self):
+    def _post(self):
+        """Everything of a cycle after the Fock build (F holds base + G)."""
         torch = self.torch
         r, k = self.rhf, self.k
         stream = torch.cuda.current_stream(r.device)
-        self.F.copy_(self.base)
-        r.eng.fock2e(self.D - self.Dref, o=self.F, stream=stream)
         F, D = self.F, self.D
         Eel = 0.5 * torch.sum(D * (r.H + F))
         e = r.X.T @ (F @ D @ r.S - r.S @ D @ F) @ r.X
@@ -337,11 +337,27 @@ class GraphSCF:
         self.base.copy_(F)
         self.D.copy_(Dn)
 
-    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess: str = "gwh", ncyc: int = 3, D0=None,
-            graph: bool = True):
+    def _pre(self, full: bool):
+        """The start of a cycle: F <- base (H and Dref = 0 on full builds); returns
+        the density the Fock build contracts, D - Dref."""
+        if full:
+            self.base.copy_(self.rhf.H)
+            self.Dref.zero_()
+        self.F.copy_(self.base)
+        return self.D - self.Dref
+
+    def _body(self):
+        r = self.rhf
+        stream = self.torch.cuda.current_stream(r.device)
+        dD = self._pre(False)
+        r.eng.fock2e(dD, o=self.F, stream=stream)
+        self._post()
+
+    def begin(self, guess: str = "gwh", D0=None):
+        """Guess density (or D0), SP2 step count from the guess spectrum, empty
+        DIIS history."""
         torch = self.torch
         r = self.rhf
-        t0 = time.perf_counter()
         if guess == "core":
             Fg = r.H
         else:
@@ -361,13 +377,16 @@ class GraphSCF:
         self.valid.zero_()
         self.errs.zero_()
         self.focks.zero_()
-        history = []
-        converged = False
-        for it in range(1, maxiter + 1):
-            if it < ncyc:
-                self.base.copy_(r.H)
-                self.Dref.zero_()
-            if graph and it >= ncyc:
+
+    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess: str = "gwh", ncyc: int = 3, D0=None,
+            graph: bool = True):
+        torch = self.torch
+        r = self.rhf
+        t0 = time.perf_counter()
+        st = DeviceSCFState(r, denserms=denserms, maxiter=maxiter, guess=guess, ncyc=ncyc, D0=D0, g=self)
+        while not st.done:
+            if graph and st.it + 1 >= ncyc:
+                st.it += 1
                 if self.graph is None:
                     torch.cuda.synchronize(r.device)
                     self.graph = torch.cuda.CUDAGraph()
@@ -375,20 +394,104 @@ class GraphSCF:
                         self._body()
                 self.graph.replay()
             else:
-                self._body()
-            Eel, prms, pchange, defect = (float(x) for x in self.out.cpu().numpy())
-            r.fock_builds += 1
-            if abs(defect) > 1e-9 * max(1, r.nocc) and self.sp2 < 200:
-                # the projection needs more steps for this spectrum: recapture with more
-                self.sp2 += 16
-                self.graph = None
-                self.recaptures += 1
-            history.append((it, Eel + r.Ecore, prms))
-            if it >= 3 and prms < denserms and pchange < 100 * denserms:
-                converged = True
-                break
+                dD, F = st.fock_input()
+                r.eng.fock2e(dD, o=F)
+                st.step_device()
+            st.step(self.out.cpu().numpy())
         torch.cuda.synchronize(r.device)
-        D = self.Dref.clone() if converged else self.D.clone()
-        return {"E": Eel + r.Ecore, "Eel": Eel, "Ecore": r.Ecore, "D": D, "F": self.F.clone(), "niter": it,
-                "converged": converged, "history": history, "seconds": time.perf_counter() - t0,
-                "sp2_steps": self.sp2, "graph": self.graph is not None, "recaptures": self.recaptures}
+        res = st.result()
+        res.update({"seconds": time.perf_counter() - t0, "sp2_steps": self.sp2, "graph": self.graph is not None,
+                    "recaptures": self.recaptures})
+        return res
+
+
+class DeviceSCFState:
+    """One RHF solve on the device, one Fock build at a time, with the arithmetic
+    of :class:`GraphSCF` (fixed-slot DIIS solved on the device, SP2 density): no
+    host synchronisation inside a cycle, so a server can advance many solves with
+    one batched build and ONE synchronisation per step.  The protocol of
+    :class:`SCFState`: ``fock_input`` -> (density, matrix to add G into);
+    ``step_device`` -> the cycle's (Eel, PRMS, PCHANGE, SP2 defect) on the device;
+    ``step(values)``; ``result()``."""
+
+    _pools = {}
+
+    def __init__(self, rhf, denserms=1e-6, maxiter=100, guess="gwh", ncyc=3, D0=None, maxdiis=10, g=None,
+                 graph: bool = False):
+        self.rhf = rhf
+        self.g = g if g is not None else GraphSCF(rhf, maxdiis=maxdiis)
+        # graph=True: the post-build half of a cycle is captured once and replayed
+        # (one launch per solve and step instead of some hundred)
+        self.use_graph = graph
+        self.post_graph = None
+        self.g.begin(guess, D0)
+        self.denserms, self.maxiter, self.ncyc = denserms, maxiter, ncyc
+        self.warm = D0 is not None
+        self.it = 0
+        self.done = False
+        self.converged = False
+        self.Eel = None
+        self.history = []
+
+    def fock_input(self):
+        self.it += 1
+        dD = self.g._pre(self.it < self.ncyc)
+        return dD, self.g.F
+
+    def step_device(self):
+        if not self.use_graph:
+            self.g._post()
+            return self.g.out
+        torch = self.rhf.torch
+        dev = self.rhf.device
+        if self.post_graph is None:
+            key = str(dev)
+            main = torch.cuda.current_stream(dev)
+            if key not in DeviceSCFState._pools:
+                # one memory pool for every solve's graph (they replay one after
+                # another on one stream), owned by a small anchor graph that lives
+                # as long as the process: a pool dies with its last graph
+                pool, cs = torch.cuda.graph_pool_handle(), torch.cuda.Stream(dev)
+                x = torch.zeros(1, device=dev)
+                anchor = torch.cuda.CUDAGraph()
+                cs.wait_stream(main)
+                with torch.cuda.stream(cs):
+                    anchor.capture_begin(pool=pool, capture_error_mode="thread_local")
+                    y = x + 1.0
+                    anchor.capture_end()
+                main.wait_stream(cs)
+                DeviceSCFState._pools[key] = (pool, cs, anchor, x, y)
+            pool, cs = DeviceSCFState._pools[key][:2]
+            cs.wait_stream(main)
+            gr = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(cs):
+                # thread_local: set-up threads may allocate while this thread captures
+                gr.capture_begin(pool=pool, capture_error_mode="thread_local")
+                self.g._post()
+                gr.capture_end()
+            main.wait_stream(cs)
+            self.post_graph = gr
+        self.post_graph.replay()
+        return self.g.out
+
+    def step(self, vals):
+        g, r = self.g, self.rhf
+        Eel, prms, pchange, defect = (float(x) for x in vals)
+        self.Eel = Eel
+        r.fock_builds += 1
+        self.history.append((self.it, Eel + r.Ecore, prms))
+        if abs(defect) > 1e-9 * max(1, r.nocc) and g.sp2 < 200:
+            g.sp2 += 16                 # the projection needs more steps for this spectrum
+            g.graph = None
+            self.post_graph = None
+            g.recaptures += 1
+        if self.it >= 3 and prms < self.denserms and pchange < 100 * self.denserms:
+            self.converged = self.done = True
+        elif self.it >= self.maxiter:
+            self.done = True
+
+    def result(self):
+        g, r = self.g, self.rhf
+        D = g.Dref.clone() if self.converged else g.D.clone()
+        return {"E": self.Eel + r.Ecore, "Eel": self.Eel, "Ecore": r.Ecore, "D": D, "F": g.F.clone(),
+                "niter": self.it, "converged": self.converged, "history": self.history}

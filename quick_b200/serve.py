@@ -18,9 +18,11 @@ measured once built) plus its SCF matrices -- fit beside the solves already
 running.  Latency of a request = completion time - arrival
 time; the server reports p50 / p99 beside throughput.
 
-The per-solve arithmetic is :class:`quick_b200.scf.SCFState`, the same object
-``RHF.run`` uses, and a batched Fock build equals the one-molecule build bit
-for bit, so a request's result does not depend on what else was in the batch.
+The per-solve arithmetic is :class:`quick_b200.scf.DeviceSCFState` -- that of
+the graph-captured SCF (``GraphSCF``) -- or :class:`quick_b200.scf.SCFState`, the
+eager loop of ``RHF.run``; a batched Fock build equals the one-molecule build
+bit for bit, so a request's result does not depend on what else was in the
+batch.
 
 The reference (QUICK) computes one molecule per process and has no server; the
 QM/MM step it serves is the Fortran API's ``get_quick_energy`` call with new
@@ -31,8 +33,10 @@ with the previous density reused when ``reusedmx`` is set
 from __future__ import annotations
 
 import math
+import threading
 import time
 from collections import deque
+from concurrent.futures import FIRST_COMPLETED, ThreadPoolExecutor, wait
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -162,6 +166,32 @@ def request_bytes_estimate(basis, maxdiis: int = 10) -> int:
     return context_bytes_estimate(basis) + scf_bytes(basis.nbasis, maxdiis)
 
 
+_ELEMENT_SIZES = {}
+
+
+def basis_size(mol, name: str):
+    """(nbasis, primitives summed over shells) of ``mol`` in basis ``name``, from
+    per-element counts (no basis arrays built)."""
+    from .basis import SYMBOLS, load_basis_data
+    nfun = {"S": 1, "P": 3, "SP": 4, "D": 6, "F": 10}
+    nb = npr = 0
+    for z in mol.Z:
+        key = (name, int(z))
+        if key not in _ELEMENT_SIZES:
+            data = load_basis_data(name)[SYMBOLS[int(z)]]
+            _ELEMENT_SIZES[key] = (sum(nfun[k] for k, _ in data), sum(len(p) for _, p in data))
+        a, b = _ELEMENT_SIZES[key]
+        nb += a
+        npr += b
+    return nb, npr
+
+
+def request_bytes_estimate_mol(mol, name: str, maxdiis: int = 10) -> int:
+    """:func:`request_bytes_estimate` from the molecule and basis name."""
+    n, prims = basis_size(mol, name)
+    return (1 << 20) + 88 * prims * prims + 400 * n * n + scf_bytes(n, maxdiis)
+
+
 class _Job:
     __slots__ = ("req", "eng", "rhf", "st", "bytes", "measured", "admitted", "warm")
 
@@ -174,11 +204,20 @@ class Server:
     ``fp32_bound``: the mixed form's Schwarz bound product below which quartets
     run in FP32 (0 = plain FP64).  ``max_active``: cap on solves in one batch.
     ``pool``: retired contexts kept for the next requests (their device buffers
-    are reused by ``Get2e.bind``; allocation and release synchronise the GPU)."""
+    are reused by ``Get2e.bind``; allocation and release synchronise the GPU).
+    ``workers``: threads that set new requests up (basis, context, pair tables,
+    one-electron integrals, guess) on their own CUDA streams while the batch
+    steps go on; 0 sets them up inline, so that every request admitted at a step
+    is in that step's batch.
+    ``scf``: "device" advances each solve with :class:`DeviceSCFState` (DIIS on
+    the device, SP2 density: no host synchronisation inside a step; the
+    post-build half of its cycle captured once as a CUDA graph); "eigh" with
+    :class:`SCFState` (torch eigh, one synchronisation per solve and step)."""
 
     def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
                  denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
-                 max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64):
+                 max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64,
+                 workers: int = 2, scf: str = "device"):
         import torch
         from .get2e import Get2eBatch
         self.torch = torch
@@ -209,57 +248,77 @@ class Server:
         self.timers = {"admit": 0.0, "setup_engine": 0.0, "setup_rhf": 0.0, "fock": 0.0, "scf": 0.0, "sync": 0.0,
                        "retire": 0.0, "fock_gpu": 0.0}
         self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        # set-up of new requests runs on its own stream, beside the batch's builds
-        self.setup_stream = torch.cuda.Stream(device)
+        # set-up of new requests runs on its own streams, beside the batch's builds
         self.main_stream = torch.cuda.current_stream(device)
+        self.workers = workers
+        self.scf = scf
+        self.executor = ThreadPoolExecutor(max_workers=workers) if workers > 0 else None
+        self._tls = threading.local()
+        self.setting_up = []          # (future, request, reserved bytes, admission time)
 
     # -- admission
-    def _engine(self, basis):
-        from .get2e import Get2e
-        if self.pool:
-            eng, b = self.pool.pop()
-            self.used -= b
-            eng.bind(basis)
-            return eng
-        eng = Get2e(basis, device=self.device, integral_cutoff=self.integral_cutoff,
-                    prim_limit=0.1 * self.integral_cutoff)
-        if self.fp32_bound > 0.0:
-            eng.set_precision(self.fp32_bound)
-        return eng
+    def _stream(self):
+        st = getattr(self._tls, "stream", None)
+        if st is None:
+            self.torch.cuda.set_device(self.device)
+            st = self._tls.stream = self.torch.cuda.Stream(self.device)
+        return st
 
-    def _setup(self, req, basis, now):
-        from .scf import RHF
+    def _setup(self, req, eng, D0):
+        """Set one request up (worker thread or inline): returns the context, the
+        RHF object, the SCF state and an event marking the end of its GPU work."""
+        from .get2e import Get2e
+        from .scf import RHF, DeviceSCFState
+        torch = self.torch
+        stream = self._stream()
         t = time.perf_counter()
-        eng = self._engine(basis)
+        basis = build_basis(req.mol, req.basis)
+        if eng is None:
+            eng = Get2e(basis, device=self.device, integral_cutoff=self.integral_cutoff,
+                        prim_limit=0.1 * self.integral_cutoff)
+            if self.fp32_bound > 0.0:
+                eng.set_precision(self.fp32_bound)
+        else:
+            eng.bind(basis)
         eng.prepare()
         t1 = time.perf_counter()
-        with self.torch.cuda.stream(self.setup_stream):
+        with torch.cuda.stream(stream):
             rhf = RHF(basis, device=self.device, ext_charges=req.ext_charges, engine=eng)
-            D0 = self.series_D.get(req.series) if req.series is not None else None
-            st = rhf.state(denserms=self.denserms, maxiter=self.maxiter, maxdiis=self.maxdiis, D0=D0)
+            if self.scf == "device":
+                st = DeviceSCFState(rhf, denserms=self.denserms, maxiter=self.maxiter, D0=D0, maxdiis=self.maxdiis,
+                                    graph=True)
+            else:
+                st = rhf.state(denserms=self.denserms, maxiter=self.maxiter, maxdiis=self.maxdiis, D0=D0)
+            ev = torch.cuda.Event()
+            ev.record(stream)
         self.timers["setup_engine"] += t1 - t
         self.timers["setup_rhf"] += time.perf_counter() - t1
+        return eng, rhf, st, ev
+
+    def _join(self, req, est, admitted, result):
+        eng, rhf, st, ev = result
+        self.main_stream.wait_event(ev)
         j = _Job()
-        j.req, j.eng, j.rhf = req, eng, rhf
-        j.warm = D0 is not None
-        j.st = st
-        j.admitted = now
+        j.req, j.eng, j.rhf, j.st = req, eng, rhf, st
+        j.warm = st.warm
+        j.admitted = admitted
         j.measured = False
-        return j
+        j.bytes = est
+        self.active.append(j)
 
     def _admit(self, now):
         """First come, first served among the admissible requests: a QM/MM repeat
         waits (without holding up the others) while its series has a request in
-        flight, so that it starts from that request's density."""
+        flight, so that it starts from that request's density.  Memory is reserved
+        here, before the set-up allocates anything."""
         t = time.perf_counter()
         skipped = deque()
-        while self.queue and len(self.active) < self.max_active:
+        while self.queue and len(self.active) + len(self.setting_up) < self.max_active:
             req = self.queue[0]
             if req.series is not None and req.series in self.series_busy:
                 skipped.append(self.queue.popleft())
                 continue
-            basis = build_basis(req.mol, req.basis)
-            est = request_bytes_estimate(basis, self.maxdiis)
+            est = request_bytes_estimate_mol(req.mol, req.basis, self.maxdiis)
             if est > self.budget:
                 self.queue.popleft()
                 self.rejected.append((req.rid, est))
@@ -268,19 +327,40 @@ class Server:
                 eng, b = self.pool.pop(0)
                 self.used -= b
                 eng.close()
-            if self.used + est > self.budget and self.active:
+            if self.used + est > self.budget and (self.active or self.setting_up):
                 break                      # wait for memory
             self.queue.popleft()
-            j = self._setup(req, basis, now)
-            j.bytes = est
+            eng = None
+            if self.pool:
+                eng, b = self.pool.pop()
+                self.used -= b
             self.used += est
             self.peak_used = max(self.peak_used, self.used)
-            self.active.append(j)
+            D0 = self.series_D.get(req.series) if req.series is not None else None
             if req.series is not None:
                 self.series_busy.add(req.series)
+            if self.executor is None:
+                self._join(req, est, now, self._setup(req, eng, D0))
+            else:
+                self.setting_up.append((self.executor.submit(self._setup, req, eng, D0), req, est, now))
         while skipped:
             self.queue.appendleft(skipped.pop())
         self.timers["admit"] += time.perf_counter() - t
+
+    def _collect(self, block_until: float = None):
+        """Requests whose set-up finished join the batch (optionally waiting up to
+        ``block_until`` seconds for the first one)."""
+        if not self.setting_up:
+            return
+        if block_until is not None:
+            wait([f for f, _, _, _ in self.setting_up], timeout=max(0.0, block_until), return_when=FIRST_COMPLETED)
+        keep = []
+        for f, req, est, adm in self.setting_up:
+            if f.done():
+                self._join(req, est, adm, f.result())
+            else:
+                keep.append((f, req, est, adm))
+        self.setting_up = keep
 
     # -- one step of every active solve, in two halves: the batched Fock build is
     # enqueued first, new requests are set up on the host and the side stream
@@ -358,23 +438,32 @@ class Server:
         clock = lambda: time.perf_counter() - t0  # noqa: E731
         self._arrival = arrival
         results = []
-        while pending or self.queue or self.active:
+        while pending or self.queue or self.active or self.setting_up:
             now = clock()
             while pending and arrival(pending[0]) <= now:
                 self.queue.append(pending.popleft())
             act = self._launch() if self.active else None
-            n_before = len(self.active)
             self._admit(now)
-            if len(self.active) > n_before:
-                self.main_stream.wait_stream(self.setup_stream)
             if act:
                 results.extend(self._finish(act, clock))
-            elif not self.active and pending:
-                time.sleep(max(0.0, arrival(pending[0]) - clock()))
+            if not self.active:
+                nxt = (arrival(pending[0]) - clock()) if pending else None
+                if self.setting_up:
+                    self._collect(block_until=nxt if nxt is not None else 60.0)
+                elif nxt is not None and not self.queue:
+                    time.sleep(max(0.0, nxt))
+            else:
+                self._collect()
         self.wall = clock()
         return sorted(results, key=lambda r: r.rid)
 
     def close(self):
+        if self.executor is not None:
+            self.executor.shutdown(wait=True)
+            for f, _, _, _ in self.setting_up:
+                if f.done() and f.exception() is None:
+                    f.result()[0].close()
+            self.setting_up = []
         for j in self.active:
             j.eng.close()
         for eng, _ in self.pool:

@@ -85,3 +85,11 @@ def test_summarize_percentiles():
     s = summarize(rs, wall=2.0)
     assert s["requests"] == 100 and s["solves_per_s"] == 50.0
     assert math.isclose(s["p50_ms"], 50.5) and math.isclose(s["p99_ms"], 99.01)
+
+
+def test_molecule_only_estimate_matches_basis():
+    from quick_b200.serve import basis_size, request_bytes_estimate, request_bytes_estimate_mol
+    for r in request_stream(20, rate=100.0, seed=12):
+        b = build_basis(r.mol, r.basis)
+        assert basis_size(r.mol, r.basis) == (b.nbasis, int(b.kprim.sum()))
+        assert request_bytes_estimate_mol(r.mol, r.basis) == request_bytes_estimate(b)

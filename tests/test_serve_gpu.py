@@ -36,7 +36,7 @@ def _mix():
 def test_alone_equals_in_mix():
     _cuda()
     reqs = _mix()
-    srv = Server(keep_densities=True)
+    srv = Server(keep_densities=True, workers=0)
     mixed = srv.serve(reqs, realtime=False)
     assert max(srv.batch_sizes) == len(reqs)        # all were in one batch at the start
     srv.close()
@@ -51,17 +51,25 @@ def test_alone_equals_in_mix():
         assert torch.equal(m.D, alone.D), r.rid
 
 
-def test_server_matches_rhf_run():
+def test_server_matches_one_molecule_solves():
+    """Device SCF in the server = GraphSCF eager, bit for bit; eigh SCF in the
+    server = RHF.run; the two agree to 1e-9 Eh."""
     _cuda()
-    from quick_b200.scf import RHF
+    from quick_b200.scf import RHF, GraphSCF
     reqs = _mix()[:3]
     srv = Server()
     got = srv.serve(reqs, realtime=False)
     srv.close()
-    for r, g in zip(reqs, got):
-        ref = RHF(build_basis(r.mol, r.basis), integral_cutoff=1e-10, ext_charges=r.ext_charges).run(denserms=1e-6)
-        assert g.niter == ref["niter"]
-        assert abs(g.E - ref["E"]) < 1e-10
+    srv = Server(scf="eigh")
+    got_e = srv.serve(reqs, realtime=False)
+    srv.close()
+    for r, g, ge in zip(reqs, got, got_e):
+        b = build_basis(r.mol, r.basis)
+        ref = GraphSCF(RHF(b, integral_cutoff=1e-10, ext_charges=r.ext_charges)).run(denserms=1e-6, graph=False)
+        assert g.niter == ref["niter"] and g.E == ref["E"]
+        ref_e = RHF(b, integral_cutoff=1e-10, ext_charges=r.ext_charges).run(denserms=1e-6)
+        assert ge.niter == ref_e["niter"] and abs(ge.E - ref_e["E"]) < 1e-10
+        assert abs(g.E - ge.E) < 1e-9
 
 
 def test_memory_budget_admission():
@@ -137,6 +145,19 @@ def test_mixed_precision_server_within_1_microhartree():
     b.close()
     for x, y in zip(r64, r32):
         assert abs(x.E - y.E) <= 1e-6, (x.rid, x.E, y.E)
+
+
+def test_threaded_setup_gives_the_same_results():
+    _cuda()
+    reqs = _mix()
+    a = Server(workers=0)
+    r0 = a.serve(reqs, realtime=False)
+    a.close()
+    b = Server(workers=3)
+    r1 = b.serve(reqs, realtime=False)
+    b.close()
+    for x, y in zip(r0, r1):
+        assert x.E == y.E and x.niter == y.niter
 
 
 def test_realtime_stream_reports_latency():
