@@ -372,24 +372,29 @@ def run_ours(args):
         from quick_b200.scf import GraphSCF
         # eager loop (torch eigh per cycle), then the graph-captured iteration (SP2 density)
         rhf = RHF(basis, device=local, engine=eng)
-        rhf.run(denserms=1e-7)
-        r2 = rhf.run(denserms=1e-7)
+        rhf.run(denserms=1e-7, guess="sad")
+        r2 = rhf.run(denserms=1e-7, guess="sad")
         gs = GraphSCF(RHF(basis, device=local, engine=eng))
-        gs.run(denserms=1e-7)                 # first run captures the graph
-        g2 = gs.run(denserms=1e-7)
-        scf = {"solves_per_s": round(1.0 / g2["seconds"], 4), "seconds": round(g2["seconds"], 3),
-               "iterations": g2["niter"], "E": g2["E"], "converged": bool(g2["converged"]),
-               "denserms": 1e-7, "incremental_builds": True,
-               "path": "one CUDA graph per SCF cycle (Fock build, DIIS, SP2 density)",
-               "sp2_steps": g2["sp2_steps"],
-               "eager_eigh": {"solves_per_s": round(1.0 / r2["seconds"], 4), "iterations": r2["niter"],
-                              "E": r2["E"]},
+        gs.run(denserms=1e-7, guess="sad")    # first run captures the graph
+        g2 = gs.run(denserms=1e-7, guess="sad")
+        # headline: the faster of the two paths on this molecule (eigh wins on tiny ones,
+        # where SP2's fixed number of small GEMMs costs more than one eigh)
+        graph_rate, eager_rate = 1.0 / g2["seconds"], 1.0 / r2["seconds"]
+        best = g2 if graph_rate >= eager_rate else r2
+        scf = {"solves_per_s": round(max(graph_rate, eager_rate), 4), "seconds": round(best["seconds"], 3),
+               "iterations": best["niter"], "E": best["E"], "converged": bool(best["converged"]),
+               "denserms": 1e-7, "incremental_builds": True, "guess": "SAD",
+               "path": ("one CUDA graph per SCF cycle (Fock build, DIIS, SP2 density)" if best is g2
+                        else "eager cycle (torch eigh per cycle)"),
+               "graph_sp2": {"solves_per_s": round(graph_rate, 4), "iterations": g2["niter"], "E": g2["E"],
+                             "sp2_steps": g2["sp2_steps"]},
+               "eager_eigh": {"solves_per_s": round(eager_rate, 4), "iterations": r2["niter"], "E": r2["E"]},
                "abs_dE_graph_vs_eager": abs(g2["E"] - r2["E"])}
         if mixed is not None:
             eng.set_precision(args.fp32_bound)
             gm = GraphSCF(RHF(basis, device=local, engine=eng))
-            gm.run(denserms=1e-7)
-            r3 = gm.run(denserms=1e-7)
+            gm.run(denserms=1e-7, guess="sad")
+            r3 = gm.run(denserms=1e-7, guess="sad")
             eng.set_precision(0.0)
             mixed["scf"] = {"solves_per_s": round(1.0 / r3["seconds"], 4), "iterations": r3["niter"],
                             "E": r3["E"], "abs_dE_vs_fp64": abs(r3["E"] - g2["E"]),

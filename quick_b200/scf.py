@@ -4,6 +4,8 @@ The caller of the hot path, restated on the GPU: QUICK's ``electdiis`` +
 ``scf_operator`` (``src/modules/quick_scf_module.f90:165-802``,
 ``src/modules/quick_scf_operator_module.f90:26-250``):
 
+* the starting density is QUICK's default SAD guess (``quick_b200.guess``;
+  "gwh" and "core" are available);
 * H = T + V from the device one-electron integrals (``qk_oei_host``);
 * symmetric orthogonalisation X = S^-1/2 (``fullx``);
 * each iteration F = H + G(D) through ``Get2e.fock2e``; from cycle ``ncyc``
@@ -95,6 +97,11 @@ class RHF:
         return 2.0 * C @ C.T
 
     def guess(self, kind="gwh"):
+        """Initial density: "core" (H), "gwh" (generalised Wolfsberg-Helmholz) or
+        "sad" (superposition of atomic densities, quick_b200.guess)."""
+        if kind == "sad":
+            from .guess import sad_density
+            return self.torch.tensor(sad_density(self.basis, self.device.index or 0), device=self.device)
         if kind == "core":
             return self.density(self.H)
         d = self.torch.diagonal(self.H)
@@ -103,12 +110,12 @@ class RHF:
         F0 += self.torch.diag(d)
         return self.density(F0)
 
-    def state(self, denserms: float = 1e-6, maxiter: int = 100, guess="gwh", incremental: bool = True,
+    def state(self, denserms: float = 1e-6, maxiter: int = 100, guess="sad", incremental: bool = True,
               ncyc: int = 3, maxdiis: int = 10, D0=None):
         """A solve that advances one Fock build at a time (:class:`SCFState`)."""
         return SCFState(self, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0)
 
-    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess="gwh", incremental: bool = True,
+    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess="sad", incremental: bool = True,
             ncyc: int = 3, maxdiis: int = 10, D0=None, verbose=False):
         t0 = time.perf_counter()
         st = self.state(denserms, maxiter, guess, incremental, ncyc, maxdiis, D0)
@@ -353,11 +360,13 @@ class GraphSCF:
         r.eng.fock2e(dD, o=self.F, stream=stream)
         self._post()
 
-    def begin(self, guess: str = "gwh", D0=None):
+    def begin(self, guess: str = "sad", D0=None):
         """Guess density (or D0), SP2 step count from the guess spectrum, empty
         DIIS history."""
         torch = self.torch
         r = self.rhf
+        if guess == "sad" and D0 is None:
+            D0 = r.guess("sad")
         if guess == "core":
             Fg = r.H
         else:
@@ -378,7 +387,7 @@ class GraphSCF:
         self.errs.zero_()
         self.focks.zero_()
 
-    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess: str = "gwh", ncyc: int = 3, D0=None,
+    def run(self, denserms: float = 1e-6, maxiter: int = 100, guess: str = "sad", ncyc: int = 3, D0=None,
             graph: bool = True):
         torch = self.torch
         r = self.rhf
@@ -416,7 +425,7 @@ class DeviceSCFState:
 
     _pools = {}
 
-    def __init__(self, rhf, denserms=1e-6, maxiter=100, guess="gwh", ncyc=3, D0=None, maxdiis=10, g=None,
+    def __init__(self, rhf, denserms=1e-6, maxiter=100, guess="sad", ncyc=3, D0=None, maxdiis=10, g=None,
                  graph: bool = False):
         self.rhf = rhf
         self.g = g if g is not None else GraphSCF(rhf, maxdiis=maxdiis)
@@ -456,6 +465,11 @@ class DeviceSCFState:
                 anchor = torch.cuda.CUDAGraph()
                 cs.wait_stream(main)
                 with torch.cuda.stream(cs):
+                    # this thread's cuBLAS handle and the stream's workspace are
+                    # created outside any capture
+                    w = torch.ones((2, 4, 4), dtype=torch.float64, device=dev)
+                    torch.einsum("k,kij->ij", w[:, 0, 0], w) @ w[0]
+                    torch.cuda.synchronize(dev)
                     anchor.capture_begin(pool=pool, capture_error_mode="thread_local")
                     y = x + 1.0
                     anchor.capture_end()
