@@ -32,6 +32,11 @@ from . import _native
 from ._native import check, lib
 from .get2e import Get2e
 
+# QUICK's level-shift controls (quick_method_module.f90:96-98): allowed from cycle
+# 3 when the largest DIIS error element exceeds 0.1 and the HOMO-LUMO gap is
+# below 0.2, which is then opened to 0.2.
+LSHIFT_CYCLE, LSHIFT_ERR, LSHIFT_GAP = 3, 0.1, 0.2
+
 
 def oei(basis, ext_charges=None, device=0):
     """S, T, V (nbasis^2 numpy) computed on the GPU."""
@@ -161,6 +166,8 @@ class SCFState:
         self.D = D0.clone() if D0 is not None else rhf.guess(guess)
         self.errs, self.focks = [], []
         self.F = self.F_prev = self.D_prev = self.Dn = None
+        self.vec, self.gap = None, None    # previous eigenvectors (orthogonal basis), HOMO-LUMO gap
+        self.shifts = 0
         self.it = 0
         self.done = False
         self.converged = False
@@ -199,7 +206,27 @@ class SCFState:
         Fd = torch.einsum("k,kij->ij", sol[:nd], torch.stack(self.focks))
         ok = (info == 0) & torch.isfinite(Fd).all()
         Fd = torch.where(ok, Fd, F)
-        self.Dn = r.density(Fd)
+        # new density: diagonalise X^T Fd X, level-shifted as QUICK does
+        # (quick_scf_module.f90:620-680): in the basis of the previous eigenvectors
+        # the virtual levels move up by (0.2 - gap)
+        Fo = r.X.T @ Fd @ r.X
+        shift = 0.0
+        if self.it >= LSHIFT_CYCLE and self.vec is not None and self.gap < LSHIFT_GAP:
+            if float(torch.abs(err).max()) > LSHIFT_ERR:
+                shift = LSHIFT_GAP - self.gap
+        if shift > 0.0:
+            Fo = self.vec.T @ Fo @ self.vec
+            v = torch.arange(r.nocc, Fo.shape[0], device=r.device)
+            Fo[v, v] += shift
+            self.shifts += 1
+        e, V = torch.linalg.eigh(Fo)
+        if shift > 0.0:
+            V = self.vec @ V
+        self.vec = V
+        ev = e[r.nocc - 1: r.nocc + 1].cpu() if r.nocc < e.shape[0] else None
+        self.gap = float(ev[1] - ev[0]) if ev is not None else 1.0
+        Co = r.X @ V[:, : r.nocc]
+        self.Dn = 2.0 * Co @ Co.T
         dD = self.Dn - D
         return torch.stack([Eel, torch.sqrt(torch.mean(dD * dD)), torch.abs(dD).max()])
 
@@ -287,16 +314,24 @@ class GraphSCF:
         self.eye_k = torch.eye(k, dtype=dt, device=dev)
         self.eye_m = torch.eye(m, dtype=dt, device=dev)
         self.out = z(4)
+        self.cycle = torch.zeros((), dtype=torch.int64, device=dev)
+        self.XtS = rhf.X.T @ rhf.S          # orthogonal-basis projector of D: (XtS) D (XtS)^T / 2
         self.zero = torch.zeros((), dtype=dt, device=dev)
         self.minus_one = torch.full((), -1.0, dtype=dt, device=dev)
+        self.lshift = torch.full((), LSHIFT_GAP, dtype=dt, device=dev)
         self.recaptures = 0
         self.sp2 = sp2
         self.graph = None
 
-    def _density(self, Fd):
+    def _density(self, Fd, shift=None):
         torch = self.torch
         X = self.rhf.X
         Fo = X.T @ Fd @ X
+        if shift is not None:
+            # level shift on the device: the virtual space of the current density
+            # moves up by `shift` (0 when no shift is due)
+            P = 0.5 * (self.XtS @ self.D @ self.XtS.T)
+            Fo = Fo + shift * (self.eye_m - P)
         d = torch.diagonal(Fo)
         rad = torch.abs(Fo).sum(dim=1) - torch.abs(d)
         emin, emax = torch.min(d - rad), torch.max(d + rad)
@@ -317,7 +352,11 @@ class GraphSCF:
         stream = torch.cuda.current_stream(r.device)
         F, D = self.F, self.D
         Eel = 0.5 * torch.sum(D * (r.H + F))
-        e = r.X.T @ (F @ D @ r.S - r.S @ D @ F) @ r.X
+        err = F @ D @ r.S - r.S @ D @ F
+        e = r.X.T @ err @ r.X
+        self.cycle.add_(1)
+        shift = torch.where((self.cycle >= LSHIFT_CYCLE) & (torch.abs(err).max() > LSHIFT_ERR),
+                            self.lshift, self.zero)
         self.errs.copy_(torch.roll(self.errs, -1, 0))
         self.errs[k - 1].copy_(e)
         self.focks.copy_(torch.roll(self.focks, -1, 0))
@@ -335,7 +374,7 @@ class GraphSCF:
                                    ctypes.c_void_p(stream.cuda_stream)), "qk_small_solve")
         Fd = torch.einsum("k,kij->ij", self.c[:k], self.focks)
         Fd = torch.where((self.ok[0] == 1) & torch.isfinite(Fd).all(), Fd, F)
-        Dn = self._density(Fd)
+        Dn = self._density(Fd, shift)
         dd = Dn - D
         self.out[0].copy_(Eel)
         self.out[1].copy_(torch.sqrt(torch.mean(dd * dd)))
@@ -384,6 +423,7 @@ class GraphSCF:
             Co = r.X @ C[:, : r.nocc]
             self.D.copy_(2.0 * Co @ Co.T)
         self.valid.zero_()
+        self.cycle.zero_()
         self.errs.zero_()
         self.focks.zero_()
 

@@ -86,21 +86,40 @@ def cluster_box(n: int) -> float:
     return max(6.0, 3.15 * n ** (1.0 / 3.0))
 
 
-def _point_charges(rng, qm_xyz_bohr, n, radius_ang, exclude_ang=2.5):
-    """n TIP3P-type charges (O, H, H, O, ...) uniform in a sphere of ``radius_ang``
-    around the QM centroid, at least ``exclude_ang`` from every QM atom."""
+def _point_charges(rng, qm_xyz_bohr, n, radius_ang, exclude_ang=2.0):
+    """n TIP3P point charges around the QM centroid: n // 3 rigid TIP3P waters
+    (O -0.834 e, two H +0.417 e; O-H 0.9572 A, H-O-H 104.52 deg) with their O
+    uniform in a sphere of ``radius_ang`` and random orientations, plus n % 3 lone
+    O charges; every charge at least ``exclude_ang`` from every QM atom.  MM
+    waters may overlap one another (they are only charges)."""
+    from .molecules import _rand_rotation
     c = qm_xyz_bohr.mean(axis=0)
     R = radius_ang * A_TO_BOHRS
-    ex = exclude_ang * A_TO_BOHRS
-    pos = []
+    ex2 = (exclude_ang * A_TO_BOHRS) ** 2
+    r, ang = 0.9572 * A_TO_BOHRS, math.radians(104.52)
+    local = np.array([[0.0, 0.0, 0.0],
+                      [r * math.sin(ang / 2), 0.0, r * math.cos(ang / 2)],
+                      [-r * math.sin(ang / 2), 0.0, r * math.cos(ang / 2)]])
+    nw, nlone = n // 3, n % 3
+    pos, q = [], []
+
+    def far(x):
+        return ((x[:, None, :] - qm_xyz_bohr[None, :, :]) ** 2).sum(-1).min() >= ex2
+
+    while len(pos) < 3 * nw:
+        o = rng.uniform(-R, R, size=3)
+        if o @ o > R * R:
+            continue
+        w = c + o + local @ _rand_rotation(rng).T
+        if far(w):
+            pos.extend(w)
+            q.extend([TIP3P_O, TIP3P_H, TIP3P_H])
     while len(pos) < n:
-        v = rng.uniform(-R, R, size=(4 * n, 3))
-        v = v[np.einsum("ij,ij->i", v, v) <= R * R] + c
-        d2 = ((v[:, None, :] - qm_xyz_bohr[None, :, :]) ** 2).sum(-1).min(axis=1)
-        pos.extend(v[d2 >= ex * ex])
-    pos = np.array(pos[:n])
-    q = np.where(np.arange(n) % 3 == 0, TIP3P_O, TIP3P_H)
-    return pos, q
+        o = rng.uniform(-R, R, size=3)
+        if o @ o <= R * R and far((c + o)[None, :]):
+            pos.append(c + o)
+            q.append(TIP3P_O)
+    return np.array(pos), np.array(q)
 
 
 def request_stream(n_requests: int, rate: float, seed: int = 20261203, qmmm_fraction: float = 0.25,
@@ -113,10 +132,10 @@ def request_stream(n_requests: int, rate: float, seed: int = 20261203, qmmm_frac
     * molecules: seeded water clusters with N log-uniform in [1, max_waters]
       (box from :func:`cluster_box`), basis uniform over ``bases``;
     * a ``qmmm_fraction`` of requests are QM/MM repeats: ``n_series`` series,
-      each a ``qm_waters`` QM region with ``n_charges`` TIP3P-type point charges
-      within ``charge_radius`` A; every repeat moves the QM atoms and the charges
-      of its series by Gaussian ``sigma`` A (a random walk), and is solved from
-      the series' last density.
+      each a ``qm_waters`` QM region with ``n_charges`` TIP3P point charges (MM
+      waters, :func:`_point_charges`) within ``charge_radius`` A; every repeat
+      moves the QM atoms and the charges of its series by Gaussian ``sigma`` A (a
+      random walk), and is solved from the series' last density.
     """
     rng = np.random.Generator(np.random.PCG64(seed))
     series = []

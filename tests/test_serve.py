@@ -54,9 +54,15 @@ def test_qmmm_series_random_walk_and_charges():
         pos, q = rs[0].ext_charges
         assert np.allclose(q[0::3], TIP3P_O) and np.allclose(q[1::3], TIP3P_H)
         c = rs[0].mol.xyz.mean(axis=0)
-        assert np.max(np.linalg.norm(pos - c, axis=1)) <= 15.0 * A_TO_BOHRS * 1.01
+        # O inside 15 A; an H can reach one O-H bond further
+        assert np.max(np.linalg.norm(pos[0::3] - c, axis=1)) <= 15.0 * A_TO_BOHRS * 1.01
+        assert np.max(np.linalg.norm(pos - c, axis=1)) <= 16.0 * A_TO_BOHRS
         dmin = np.min(np.linalg.norm(pos[:, None, :] - rs[0].mol.xyz[None], axis=2))
-        assert dmin >= 2.4 * A_TO_BOHRS
+        assert dmin >= 1.9 * A_TO_BOHRS
+        # rigid TIP3P waters (one random-walk step of 0.01 A away from 0.9572 A)
+        oh = np.linalg.norm(pos[1::3][:1300] - pos[0::3][:1300], axis=1) / A_TO_BOHRS
+        assert abs(np.median(oh) - 0.9572) < 0.02
+        assert abs(q.sum() - TIP3P_O) < 1e-12          # 1333 neutral waters + one O charge
 
 
 def test_stream_is_seeded():
