@@ -167,8 +167,60 @@ class QuickBasis:
         return int((self.qfinal - self.qstart + 1).sum())
 
 
+_ELEMENT_TEMPLATES = {}
+
+
 def build_basis(mol: Molecule, name: str) -> QuickBasis:
-    """Assemble QUICK's basis arrays for ``mol`` (src/basis.f90:389-830)."""
+    """QUICK's basis arrays for ``mol`` (src/basis.f90:389-830), assembled from
+    per-element templates: every array of a molecule is the concatenation of its
+    atoms' blocks (an atom's shells, functions and primitives are contiguous and
+    their normalisation involves only that atom), so each element's block is
+    computed once by :func:`_build_basis_direct` and reused with offsets."""
+    i32 = np.int32
+    parts = []
+    for z in mol.Z:
+        key = (name, int(z))
+        t = _ELEMENT_TEMPLATES.get(key)
+        if t is None:
+            t = _build_basis_direct(Molecule(Z=np.array([int(z)], dtype=np.int32), xyz=np.zeros((1, 3))), name)
+            _ELEMENT_TEMPLATES[key] = t
+        parts.append(t)
+    b = QuickBasis(mol=mol, name=name)
+    b.nshell = sum(t.nshell for t in parts)
+    b.nbasis = sum(t.nbasis for t in parts)
+    b.jbasis = sum(t.jbasis for t in parts)
+    b.nprim = sum(t.nprim for t in parts)
+    b.maxcontract = max(t.maxcontract for t in parts)
+    b.has_f = any(t.has_f for t in parts)
+    jb = np.cumsum([0] + [t.jbasis for t in parts])
+    nb = np.cumsum([0] + [t.nbasis for t in parts])
+    cat = np.concatenate
+    b.kstart = cat([t.kstart + jb[a] for a, t in enumerate(parts)]).astype(i32)
+    b.katom = cat([np.full(t.nshell, a + 1, dtype=i32) for a, t in enumerate(parts)])
+    for f in ("ktype", "kprim", "qnumber", "qstart", "qfinal"):
+        setattr(b, f, cat([getattr(t, f) for t in parts]).astype(i32))
+    b.qsbasis = cat([t.qsbasis for t in parts]).astype(i32)
+    b.qfbasis = cat([t.qfbasis for t in parts]).astype(i32)
+    b.ksumtype = cat([t.ksumtype[:-1] + nb[a] for a, t in enumerate(parts)] +
+                     [np.array([b.nbasis + 1])]).astype(i32)
+    b.gccoeff = np.concatenate([t.gccoeff for t in parts], axis=1)
+    b.gcexpo = np.concatenate([t.gcexpo for t in parts], axis=1)
+    b.cons = cat([t.cons for t in parts])
+    b.klmn = np.concatenate([t.klmn for t in parts], axis=1).astype(i32)
+    b.aex = cat([t.aex for t in parts])
+    b.ncenter = cat([np.full(t.nbasis, a + 1, dtype=i32) for a, t in enumerate(parts)])
+    b.ncontract = cat([t.ncontract for t in parts]).astype(i32)
+    b.itype = np.concatenate([t.itype for t in parts], axis=1).astype(i32)
+    b.aexp = np.zeros((b.maxcontract, b.nbasis))
+    b.dcoeff = np.zeros((b.maxcontract, b.nbasis))
+    for a, t in enumerate(parts):
+        b.aexp[:t.maxcontract, nb[a]:nb[a + 1]] = t.aexp
+        b.dcoeff[:t.maxcontract, nb[a]:nb[a + 1]] = t.dcoeff
+    return b
+
+
+def _build_basis_direct(mol: Molecule, name: str) -> QuickBasis:
+    """Assemble QUICK's basis arrays for ``mol`` shell by shell (src/basis.f90:389-830)."""
     data = load_basis_data(name)
     shells = []   # (atom_index0, kind, prims)
     for ia, z in enumerate(mol.Z):
