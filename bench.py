@@ -313,6 +313,7 @@ def run_ours(args):
             "ms_alone": round(float(cls_ms[i]), 4),
             "share_alone": round(float(cls_ms[i] / max(cls_ms.sum(), 1e-30)), 4),
             "quartets": int(qd[i]), "prim_quartets": int(pqd[i]),
+            "quartets_listed": int(ql[i]), "prim_quartets_listed": int(pql[i]),
             "tflops": round(float(flops[i] / (cls_ms[i] * 1e-3) * 1e-12) if cls_ms[i] > 0 else 0.0, 3)}
         for i in range(nc) if ql[i] > 0}
 

@@ -340,14 +340,28 @@ def emit_class(La, Lb, Lc, Ld):
     if coop:
         rows, off, tslots = vrr_table(g, targets, M)
         o.append(f"  static constexpr int NNODE = {len(rows)}, NLEVEL = {len(off) - 1}, NSLOT = {M + 2 + len(rows)};")
-        o.append(f"  static __device__ const VrrNode* nodes() {{ return vrr_nodes_{tag}; }}")
-        o.append(f"  static __device__ const short* level_off() {{ return vrr_levels_{tag}; }}")
         o.append(f"  static __device__ const short* targets() {{ return vrr_targets_{tag}; }}")
-        tab = ",\n".join(f"  {{{k}, {a}, {x}, {y}, {z}, {w}, {v}, {n2!r}f, {na!r}f}}"
-                          for (k, a, x, y, z, w, v, n2, na) in rows)
-        pre = [f"__device__ const VrrNode vrr_nodes_{tag}[{len(rows)}] = {{\n{tab}\n}};",
-               f"__device__ const short vrr_levels_{tag}[{len(off)}] = {{{', '.join(map(str, off))}}};",
+        # packed node words: x = a | b << 16, y = c | d << 16, z = g | gidx << 16,
+        # w = n2 | na << 8 (gidx = kind * 3 + axis; all small non-negative integers)
+        words = []
+        for (k, a, x, y, z, w, v, n2, na) in rows:
+            assert max(x, y, z, w, v) < 65536 and float(n2).is_integer() and float(na).is_integer()
+            words.append(f"{{{x} | ({y} << 16), {z} | ({w} << 16), {v} | ({k * 3 + a} << 16), "
+                         f"{int(n2)} | ({int(na)} << 8)}}")
+        pre = [f"__device__ const int4 vrr_ops_{tag}[{len(rows)}] = {{\n  " + ",\n  ".join(words) + "\n};",
                f"__device__ const short vrr_targets_{tag}[{len(tslots)}] = {{{', '.join(map(str, tslots))}}};"]
+        # the levels as straight-line rounds of 32 nodes (a level's rounds are
+        # independent, so their loads can be issued together)
+        o.append("  static __device__ __forceinline__ void vrr_coop(double* __restrict__ V, const double* __restrict__ gs, int lane) {")
+        o.append(f"    const int4* __restrict__ ops = vrr_ops_{tag};")
+        for L in range(len(off) - 1):
+            k0, k1 = off[L], off[L + 1]
+            for r0 in range(k0, k1, 32):
+                cnt = min(32, k1 - r0)
+                guard = "" if cnt == 32 else f"if (lane < {cnt}) "
+                o.append(f"    {guard}coop_node(V, gs, ops, {r0} + lane, {M + 2});")
+            o.append("    __syncwarp();")
+        o.append("  }")
         o = o[:1] + pre + o[1:]
     o.append("};")
     stats = dict(cls=tag, vrr=g.counter, hb=len(hb_lines), hk=len(hk_lines), NE=NE, NF=NF, coop=coop)
@@ -391,7 +405,19 @@ def main(out_dir, lmax=LMAX):
     parts = ["// Generated by gen_eri.py -- do not edit.",
              "#pragma once",
              "// one VRR node: kind 0 = bra step (PA, WP, oo2z, rho_z), 1 = ket step (QC, WQ, oo2e, rho_e)",
-             "struct VrrNode { unsigned char kind, axis; short a, b, c, d, g; float n2, na; };",
+             "// One node of the cooperative VRR: V[base + k] from five slots of V and the",
+             "// warp's geometry table gs (0-2 PA, 3-5 QC, 6-8 WP, 9-11 WQ, 12 1/2zeta,",
+             "// 13 1/2eta, 14 rho/zeta, 15 rho/eta, 16 1/2(zeta+eta)); one formula for",
+             "// bra (gidx 0-2) and ket (gidx 3-5) steps, unused operands on the zero slot.",
+             "__device__ __forceinline__ void coop_node(double* __restrict__ V, const double* __restrict__ gs,",
+             "                                          const int4* __restrict__ ops, int k, int base) {",
+             "  const int4 w = __ldg(ops + k);",
+             "  const int a = w.x & 0xffff, b = w.x >> 16, c = w.y & 0xffff, d = w.y >> 16;",
+             "  const int g = w.z & 0xffff, gi = w.z >> 16, kind = gi >= 3 ? 1 : 0;",
+             "  const double n2 = (double)(w.w & 0xff), na = (double)(w.w >> 8);",
+             "  const double t = n2 * gs[12 + kind] * (V[c] - gs[14 + kind] * V[d]) + na * gs[16] * V[g];",
+             "  V[base + k] = gs[gi] * V[a] + gs[6 + gi] * V[b] + t;",
+             "}",
              "template <int La, int Lb, int Lc, int Ld> struct EriClass;"]
     stats = []
     for cls in class_list(lmax):

@@ -316,7 +316,8 @@ struct CoopLayout {
     static constexpr int WORK = Cls::NSLOT > HRR ? Cls::NSLOT : HRR;
     static constexpr int DBLK = NAB + NCD + Cls::NB * Cls::ND + Cls::NA * Cls::ND + Cls::NB * Cls::NC +
                                 Cls::NA * Cls::NC;
-    static constexpr int PER_WARP = ACC + WORK + DBLK;   // doubles
+    static constexpr int GEO = 24;                       // the VRR's geometry table (17 used)
+    static constexpr int PER_WARP = ACC + WORK + DBLK + GEO;   // doubles
     // warps per block: as many as fit 227 KB of shared memory, at most 4
     static constexpr int FIT = (227 * 1024) / (8 * PER_WARP);
     static constexpr int WARPS = FIT < 1 ? 1 : (FIT > 4 ? 4 : FIT);
@@ -334,9 +335,8 @@ __device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp
     constexpr int M = Cls::M;
     for (int t = lane; t < Lay::ACC; t += 32) acc[t] = 0.0;
     if (lane == 0) V[M + 1] = 0.0;
-    const VrrNode* __restrict__ tab = Cls::nodes();
-    const short* __restrict__ loff = Cls::level_off();
     const short* __restrict__ tgt = Cls::targets();
+    double* gs = acc + Lay::PER_WARP - Lay::GEO;          // this warp's geometry table
     for (int i = 0; i < bnp; ++i) {
         const int pi = bp0 + i * bps;
         const double zeta = __ldg(d.pp_zeta + pi), oo2z = __ldg(d.pp_oo2z + pi);
@@ -355,31 +355,16 @@ __device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const double pref = Kab * __ldg(d.pp_K + pj) * rs;
-            const double oo2ze = 0.5 * inv_s;
-            const double WPx = -rho_z * PQx, WPy = -rho_z * PQy, WPz = -rho_z * PQz;
-            const double QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
-            const double WQx = rho_e * PQx, WQy = rho_e * PQy, WQz = rho_e * PQz;
             if (lane <= M) V[lane] = boys_one(lane, T, d.boys) * pref;
-            __syncwarp();
-            for (int L = 0; L < Cls::NLEVEL; ++L) {
-                const int k1 = loff[L + 1];
-                for (int k = loff[L] + lane; k < k1; k += 32) {
-                    const VrrNode nd = tab[k];
-                    double val;
-                    if (nd.kind) {
-                        const double qc = nd.axis == 0 ? QCx : (nd.axis == 1 ? QCy : QCz);
-                        const double wq = nd.axis == 0 ? WQx : (nd.axis == 1 ? WQy : WQz);
-                        val = qc * V[nd.a] + wq * V[nd.b] + nd.n2 * oo2e * (V[nd.c] - rho_e * V[nd.d]) +
-                              nd.na * oo2ze * V[nd.g];
-                    } else {
-                        const double pa = nd.axis == 0 ? PAx : (nd.axis == 1 ? PAy : PAz);
-                        const double wp = nd.axis == 0 ? WPx : (nd.axis == 1 ? WPy : WPz);
-                        val = pa * V[nd.a] + wp * V[nd.b] + nd.n2 * oo2z * (V[nd.c] - rho_z * V[nd.d]);
-                    }
-                    V[M + 2 + k] = val;
-                }
-                __syncwarp();
+            if (lane == 0) {
+                gs[0] = PAx; gs[1] = PAy; gs[2] = PAz;
+                gs[3] = Qx - Cx; gs[4] = Qy - Cy; gs[5] = Qz - Cz;
+                gs[6] = -rho_z * PQx; gs[7] = -rho_z * PQy; gs[8] = -rho_z * PQz;
+                gs[9] = rho_e * PQx; gs[10] = rho_e * PQy; gs[11] = rho_e * PQz;
+                gs[12] = oo2z; gs[13] = oo2e; gs[14] = rho_z; gs[15] = rho_e; gs[16] = 0.5 * inv_s;
             }
+            __syncwarp();
+            Cls::vrr_coop(V, gs, lane);
             for (int t = lane; t < Lay::ACC; t += 32) acc[t] += V[tgt[t]];
             __syncwarp();
         }
