@@ -236,7 +236,7 @@ class Server:
     def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
                  denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
                  max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64,
-                 workers: int = 2, scf: str = "device"):
+                 workers: int = 4, scf: str = "device"):
         import torch
         from .get2e import Get2eBatch
         self.torch = torch
@@ -351,7 +351,10 @@ class Server:
             self.queue.popleft()
             eng = None
             if self.pool:
-                eng, b = self.pool.pop()
+                # the largest kept context: its buffers most likely fit without a
+                # reallocation (cudaMalloc/cudaFree synchronise the whole GPU)
+                i = max(range(len(self.pool)), key=lambda x: self.pool[x][1])
+                eng, b = self.pool.pop(i)
                 self.used -= b
             self.used += est
             self.peak_used = max(self.peak_used, self.used)
