@@ -191,6 +191,17 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x: float, pg, device) -> float:
+    """The largest of every rank's x (the job's time is its slowest rank's); x
+    itself without a process group.  Every rank must call it at the same point."""
+    if not pg:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -260,10 +271,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = float(sum(step_ms))
-    if pg:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, pg, dev)
     ms_per_step = total_ms / args.steps
     value = world * 1000.0 / ms_per_step
 
@@ -332,11 +340,7 @@ def run_ours(args):
         on[:] = 0.0
         res = eng.fock2e_host(Dn, o=on)
         e2e_t.append(time.perf_counter() - t0)
-    e2e_total = float(sum(e2e_t))
-    if pg:
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(float(sum(e2e_t)), pg, dev)
     e2e_value = world * args.steps / e2e_total
     # parity spot check of the timed result (bitwise run-to-run identity)
     G_dev = o.cpu().numpy()

@@ -64,3 +64,14 @@ def test_class_launch_rejects_bad_shapes():
     with pytest.raises(QuickError):
         at.set_shape(eng, 10 ** 6, 1)
     eng.close()
+
+
+def test_tune_precision_stays_within_1_microhartree():
+    _cuda()
+    from quick_b200 import autotune as at
+    from quick_b200.scf import RHF
+    b = build_basis(water_cluster(3, 6.0, seed=2), "6-31G*")
+    rep = at.tune_precision(lambda: RHF(b, integral_cutoff=1e-10), bounds=(1e-6, 1e-5), reps=2)
+    assert rep["best_bound"] in (0.0, 1e-6, 1e-5)
+    for bound, row in rep["bounds"].items():
+        assert row["dE"] <= 1e-6, (bound, row)
