@@ -500,7 +500,10 @@ class DeviceSCFState:
                 # one memory pool for every solve's graph (they replay one after
                 # another on one stream), owned by a small anchor graph that lives
                 # as long as the process: a pool dies with its last graph
-                pool, cs = torch.cuda.graph_pool_handle(), torch.cuda.Stream(dev)
+                # the capture stream comes from torch's high-priority stream pool:
+                # pool streams are shared, and a normal-priority one may be another
+                # thread's current stream
+                pool, cs = torch.cuda.graph_pool_handle(), torch.cuda.Stream(dev, priority=-1)
                 x = torch.zeros(1, device=dev)
                 anchor = torch.cuda.CUDAGraph()
                 cs.wait_stream(main)

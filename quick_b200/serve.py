@@ -271,6 +271,12 @@ class Server:
         self.main_stream = torch.cuda.current_stream(device)
         self.workers = workers
         self.scf = scf
+        # torch initialises its linear-algebra back end lazily and not thread-safely:
+        # do it here, before the set-up threads call eigh / solve for the first time
+        a = torch.eye(4, dtype=torch.float64, device=torch.device("cuda", device)) * 2.0
+        torch.linalg.eigh(a)
+        torch.linalg.solve_ex(a, a[0])
+        (a @ a).sum().item()
         self.executor = ThreadPoolExecutor(max_workers=workers) if workers > 0 else None
         self._tls = threading.local()
         self.setting_up = []          # (future, request, reserved bytes, admission time)
@@ -280,7 +286,7 @@ class Server:
         st = getattr(self._tls, "stream", None)
         if st is None:
             self.torch.cuda.set_device(self.device)
-            st = self._tls.stream = self.torch.cuda.Stream(self.device)
+            st = self._tls.stream = self.torch.cuda.Stream(self.device, priority=0)
         return st
 
     def _setup(self, req, eng, D0):
