@@ -99,20 +99,26 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, const double2
     constexpr int M = Cls::M;
 #pragma unroll
     for (int i = 0; i < Cls::NE * Cls::NF; ++i) acc[i] = R(0);
-    for (int i = 0; i < bnp; ++i) {
-        const int pi = bp0 + i * bps;
-        const double zeta = __ldg(d.pp_zeta + pi);
-        const double oo2z = __ldg(d.pp_oo2z + pi);
-        const double Kab = __ldg(d.pp_K + pi) * kX0;
-        const double cut1 = dnmax * __ldg(d.pp_cut + pi);
-        const double Px = __ldg(d.pp_Px + pi), Py = __ldg(d.pp_Py + pi), Pz = __ldg(d.pp_Pz + pi);
-        const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
-        for (int j = 0; j < knp; ++j) {
-            const int pj = kp0 + j * kps;
-            if (prim_screen && !(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;
+    // ket primitive outer, bra primitive inner: the lane's own ket data is read
+    // once per ket primitive; the inner loop reads only the bra data, which is
+    // the same for the whole warp
+    for (int j = 0; j < knp; ++j) {
+        const int pj = kp0 + j * kps;
+        const double cutj = __ldg(d.pp_cut + pj);
+        const double eta = __ldg(d.pp_zeta + pj);
+        const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
+        const double Kcd = __ldg(d.pp_K + pj);
+        const double oo2e = __ldg(d.pp_oo2z + pj);
+        for (int i = 0; i < bnp; ++i) {
+            const int pi = bp0 + i * bps;
+            const double cut1 = dnmax * __ldg(d.pp_cut + pi);
+            if (prim_screen && !(cut1 * cutj > d.primLimit)) continue;
             ++*nprim_done;
-            const double eta = __ldg(d.pp_zeta + pj);
-            const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
+            const double zeta = __ldg(d.pp_zeta + pi);
+            const double oo2z = __ldg(d.pp_oo2z + pi);
+            const double Kab = __ldg(d.pp_K + pi) * kX0;
+            const double Px = __ldg(d.pp_Px + pi), Py = __ldg(d.pp_Py + pi), Pz = __ldg(d.pp_Pz + pi);
+            const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
             const double s = zeta + eta;
             const double rs = rsqrt(s);            // 1/sqrt(zeta+eta), 1 ulp
             const double inv_s = rs * rs;
@@ -120,7 +126,7 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, const double2
             const double rho = zeta * rho_z;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = Kab * __ldg(d.pp_K + pj) * rs;
+            const double pref = Kab * Kcd * rs;
             double F[M + 1];
             boys_scaled_rows<M>(T, pref, bt, F);
             VrrGeom<R> G;
@@ -129,7 +135,7 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, const double2
             G.QC[0] = R(Qx - C[0]); G.QC[1] = R(Qy - C[1]); G.QC[2] = R(Qz - C[2]);
             G.WQ[0] = R(rho_e * PQx); G.WQ[1] = R(rho_e * PQy); G.WQ[2] = R(rho_e * PQz);
             G.oo2z = R(oo2z);
-            G.oo2e = R(__ldg(d.pp_oo2z + pj));
+            G.oo2e = R(oo2e);
             G.oo2ze = R(0.5 * inv_s);
             G.rho_z = R(rho_z);
             G.rho_e = R(rho_e);
@@ -853,13 +859,16 @@ struct DevBuf {
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { if (p) cudaFree(p); }
+    // Grows by at least a quarter when it grows: a context reused for a slightly
+    // larger molecule then keeps its buffers (cudaFree synchronises the whole GPU).
     cudaError_t reserve(size_t count) {
         n = count;
         if (count <= cap && p) return cudaSuccess;
+        const size_t want = cap > 0 ? std::max(count, cap + cap / 4) : count;
         if (p) { cudaFree(p); p = nullptr; cap = 0; }
         if (count == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e == cudaSuccess) cap = count;
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e == cudaSuccess) cap = want;
         return e;
     }
     size_t bytes() const { return cap * sizeof(T); }
@@ -1009,6 +1018,9 @@ struct qk_ctx {
     cudaEvent_t ev[2 * qk::kNumClasses] = {};
     bool ev_recorded[qk::kNumClasses] = {};
     qk::DevBuf<unsigned long long> d_stats;
+    // Schwarz-bound scratch (per pair class work lists and the bit-pattern maxima)
+    qk::DevBuf<unsigned long long> d_schwarz_Y, d_schwarz_cp;
+    qk::DevBuf<int2> d_schwarz_work[(QK_MAX_L + 1) * (QK_MAX_L + 1)];
     // concurrent class launches: fork/join over auxiliary streams
     static constexpr int kAux = 4;
     cudaStream_t aux[kAux] = {};
@@ -1750,7 +1762,9 @@ int qk_schwarz(qk_ctx* c, double* Yout, double* cpout) {
         if (st) return st;
         c->pairs_dirty = true;
         const int ns = c->nshell, jb = c->jbasis;
-        DevBuf<unsigned long long> dY, dcp;
+        // scratch kept in the context: freeing device memory synchronises the whole GPU
+        DevBuf<unsigned long long>& dY = c->d_schwarz_Y;
+        DevBuf<unsigned long long>& dcp = c->d_schwarz_cp;
         QK_CUDA_TRY(dY.reserve((size_t)ns * ns));
         QK_CUDA_TRY(dcp.reserve((size_t)jb * jb));
         QK_CUDA_TRY(cudaMemsetAsync(dY.p, 0, sizeof(unsigned long long) * ns * ns, c->stream));
@@ -1766,7 +1780,7 @@ int qk_schwarz(qk_ctx* c, double* Yout, double* cpout) {
             v.push_back(make_int2(p, -1));
             for (int k = 0; k < T.npp[p]; ++k) v.push_back(make_int2(p, k));
         }
-        std::vector<DevBuf<int2>> dwl(wl.size());
+        DevBuf<int2>* dwl = c->d_schwarz_work;
 #define QK_SCHWARZ(a, b)                                                                          \
         {                                                                                         \
             auto& v = wl[a * (lmax + 1) + b];                                                     \
@@ -2090,7 +2104,7 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
                      T.d_Y.bytes(), T.d_zeta.bytes(), T.d_oo2z.bytes(), T.d_K.bytes(), T.d_cut.bytes(),
                      T.d_Px.bytes(), T.d_Py.bytes(), T.d_Pz.bytes(), T.d_PAx.bytes(), T.d_PAy.bytes(),
-                     T.d_PAz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
+                     T.d_PAz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
                      c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(),
                      c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
                      c->d_A.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
