@@ -150,8 +150,8 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, const double2
 // One quartet (bra pair P, ket pair Q): integrals, J/K digestion.
 // Lane-private updates go straight to A; the bra J block is returned in jab
 // (already weighted) for the warp reduction.
-template <int La, int Lb, int Lc, int Ld>
-__device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __restrict__ bt, int P, int Q, bool fp32,
+template <int La, int Lb, int Lc, int Ld, bool FP32>
+__device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __restrict__ bt, int P, int Q,
                                              double* jab_out, int* nq_done, int* np_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND;
@@ -174,7 +174,7 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
     const double CD[3] = {Cc[0] - d.xyz[3 * id], Cc[1] - d.xyz[3 * id + 1], Cc[2] - d.xyz[3 * id + 2]};
 
     double acc[NE * NF];
-    if (fp32) {
+    if constexpr (FP32) {
         // mixed form: small-bound quartet, vertical recursion and contraction in FP32
         float accf[NE * NF];
         contract_quartet<La, Lb, Lc, Ld, float>(d, bt, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q],
@@ -513,7 +513,9 @@ constexpr int kMaxLaneWarps = 8;
 
 // Work item: x = bra pair, y = first ket pair, z = number of kets (<= 32),
 // w = 1 for the mixed form's FP32 quartets.
-template <int La, int Lb, int Lc, int Ld>
+// FP32 = true: the mixed form's small-bound items (VRR and contraction in FP32),
+// compiled apart so that the FP64 items keep their register budget and vice versa.
+template <int La, int Lb, int Lc, int Ld, bool FP32>
 __global__ void __launch_bounds__(32 * kMaxLaneWarps)
 fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
@@ -530,7 +532,7 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, bt, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld, FP32>(d, bt, w.x, w.y + lane, jab, &nq, &np);
         if (d.stats) {
             const unsigned sq = __reduce_add_sync(0xffffffffu, (unsigned)nq);
             const unsigned sp = __reduce_add_sync(0xffffffffu, (unsigned)np);
@@ -574,7 +576,7 @@ __device__ __forceinline__ int batch_find_seg(const BatchSeg* __restrict__ segs,
     return lo;
 }
 
-template <int La, int Lb, int Lc, int Ld>
+template <int La, int Lb, int Lc, int Ld, bool FP32>
 __global__ void __launch_bounds__(32 * kMaxLaneWarps)
 fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restrict__ segs, int nseg, int n_items,
                         int* __restrict__ counter) {
@@ -594,7 +596,7 @@ fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restri
 #pragma unroll
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld>(d, bt, w.x, w.y + lane, w.w != 0, jab, &nq, &np);
+        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld, FP32>(d, bt, w.x, w.y + lane, jab, &nq, &np);
         const int P = w.x;
         const int fa = d.q_f0[d.pr_qa[P]], fb = d.q_f0[d.pr_qb[P]];
 #pragma unroll
@@ -907,36 +909,45 @@ struct PairTable {
     }
 };
 
-using FockFn = void (*)(dim3, dim3, size_t, cudaStream_t, const DevData&, const int4*, int, int*);
+using FockFn = void (*)(bool, dim3, dim3, size_t, cudaStream_t, const DevData&, const int4*, int, int*);
 template <int a, int b, int c, int e>
-void launch_fock(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData& dd, const int4* it, int n, int* cnt) {
+void launch_fock(bool fp32, dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData& dd, const int4* it, int n,
+                 int* cnt) {
     if constexpr (EriClass<a, b, c, e>::COOP)
         fock_coop_kernel<a, b, c, e><<<g, bl, smem, s>>>(dd, it, n, cnt);
+    else if (fp32)
+        fock_class_kernel<a, b, c, e, true><<<g, bl, smem, s>>>(dd, it, n, cnt);
     else
-        fock_class_kernel<a, b, c, e><<<g, bl, smem, s>>>(dd, it, n, cnt);
+        fock_class_kernel<a, b, c, e, false><<<g, bl, smem, s>>>(dd, it, n, cnt);
 }
 template <int a, int b, int c, int e>
-const void* fock_fn_ptr() {
+const void* fock_fn_ptr(bool fp32) {
     if constexpr (EriClass<a, b, c, e>::COOP)
         return (const void*)&fock_coop_kernel<a, b, c, e>;
+    else if (fp32)
+        return (const void*)&fock_class_kernel<a, b, c, e, true>;
     else
-        return (const void*)&fock_class_kernel<a, b, c, e>;
+        return (const void*)&fock_class_kernel<a, b, c, e, false>;
 }
-using FockBatchFn = void (*)(dim3, dim3, size_t, cudaStream_t, const DevData*, const BatchSeg*, int, int, int*);
+using FockBatchFn = void (*)(bool, dim3, dim3, size_t, cudaStream_t, const DevData*, const BatchSeg*, int, int, int*);
 template <int a, int b, int c, int e>
-void launch_fock_batch(dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData* dl, const BatchSeg* segs,
-                       int nseg, int n, int* cnt) {
+void launch_fock_batch(bool fp32, dim3 g, dim3 bl, size_t smem, cudaStream_t s, const DevData* dl,
+                       const BatchSeg* segs, int nseg, int n, int* cnt) {
     if constexpr (EriClass<a, b, c, e>::COOP)
         fock_coop_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
+    else if (fp32)
+        fock_class_kernel_batch<a, b, c, e, true><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
     else
-        fock_class_kernel_batch<a, b, c, e><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
+        fock_class_kernel_batch<a, b, c, e, false><<<g, bl, smem, s>>>(dl, segs, nseg, n, cnt);
 }
 template <int a, int b, int c, int e>
-const void* fock_batch_fn_ptr() {
+const void* fock_batch_fn_ptr(bool fp32) {
     if constexpr (EriClass<a, b, c, e>::COOP)
         return (const void*)&fock_coop_kernel_batch<a, b, c, e>;
+    else if (fp32)
+        return (const void*)&fock_class_kernel_batch<a, b, c, e, true>;
     else
-        return (const void*)&fock_class_kernel_batch<a, b, c, e>;
+        return (const void*)&fock_class_kernel_batch<a, b, c, e, false>;
 }
 template <int a, int b, int c, int e>
 constexpr size_t coop_smem() {
@@ -949,13 +960,13 @@ constexpr size_t coop_smem() {
 struct ClassEntry {
     int La, Lb, Lc, Ld;
     FockFn fn;
-    const void* (*kernel)();
+    const void* (*kernel)(bool fp32);
     double prim_flops, quartet_flops;   // algorithmic FP64 operations (gen_eri.py model)
     bool coop;                          // one quartet per warp (high angular momentum)
     size_t smem;                        // dynamic shared memory of a block (coop only)
     int coop_warps;                     // warps per block of the cooperative kernel
     FockBatchFn fn_batch;               // many-molecule variant
-    const void* (*kernel_batch)();
+    const void* (*kernel_batch)(bool fp32);
 };
 template <int a, int b, int c, int e>
 constexpr int coop_warps() {
@@ -978,6 +989,8 @@ struct ClassWork {
     long long nquart = 0, nprimq = 0, nquart32 = 0;
     int block = 0;        // threads per block of the class launch
     size_t smem = 0;      // dynamic shared memory of a block
+    int n64 = 0;          // items [0, n64) are FP64, [n64, size) the mixed form's FP32 ones
+    int grid32 = 0;       // grid of the FP32 launch
     int grid = 0;
 };
 
@@ -1244,13 +1257,18 @@ static int class_launch_shape(qk_ctx* c, int ci) {
     const int wpb = c->cls_wpb[ci] > 0 ? c->cls_wpb[ci] : (ce.coop ? ce.coop_warps : kWarpsPerBlock);
     const size_t smem = ce.coop ? ce.smem / ce.coop_warps * wpb : 0;
     if (smem > 48 * 1024)
-        QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
-    int bps = 0;
-    QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(), 32 * wpb, smem));
-    if (bps < 1) return fail(QK_ERR_CUDA, "class kernel cannot be resident");
-    if (c->cls_bpsm[ci] > 0) bps = std::min(bps, c->cls_bpsm[ci]);
-    const long long need = ((long long)W.items.size() + wpb - 1) / wpb;
-    W.grid = (int)std::max<long long>(1, std::min<long long>((long long)bps * c->num_sms, need));
+        QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(false), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
+    for (int part = 0; part < 2; ++part) {
+        const long long n = part == 0 ? W.n64 : (long long)W.items.size() - W.n64;
+        int& grid = part == 0 ? W.grid : W.grid32;
+        grid = 0;
+        if (n <= 0) continue;
+        int bps = 0;
+        QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(part == 1), 32 * wpb, smem));
+        if (bps < 1) return fail(QK_ERR_CUDA, "class kernel cannot be resident");
+        if (c->cls_bpsm[ci] > 0) bps = std::min(bps, c->cls_bpsm[ci]);
+        grid = (int)std::max<long long>(1, std::min<long long>((long long)bps * c->num_sms, (n + wpb - 1) / wpb));
+    }
     W.block = 32 * wpb;
     W.smem = smem;
     return QK_OK;
@@ -1312,14 +1330,20 @@ static int build_work(qk_ctx* c) {
                 }
             }
         }
-        std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) { return x.cost > y.cost; });
+        // FP64 items first, then the FP32 ones (two launches); each part by cost
+        std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) {
+            if (x.it.w != y.it.w) return x.it.w < y.it.w;
+            return x.cost > y.cost;
+        });
+        W.n64 = 0;
+        for (const Tmp& t : tmp) W.n64 += t.it.w == 0;
         W.items.resize(tmp.size());
         for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
         QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
         if (!W.items.empty()) {
             int st = class_launch_shape(c, ci);
             if (st) return st;
-            c->launches++;
+            c->launches += (W.n64 > 0) + (W.n64 < (int)W.items.size());
         }
     }
     c->launches += 1;  // finalize
@@ -1360,6 +1384,18 @@ static int ensure_pairs(qk_ctx* c) {
     return QK_OK;
 }
 
+// One class's launches: its FP64 items, then (mixed form) its FP32 items, each
+// part with its own counter (counters[ci] and counters[kNumClasses + ci]).
+static void launch_class(const ClassEntry& ce, const ClassWork& W, cudaStream_t s, const DevData& d, int* counters,
+                         int ci) {
+    const int n = (int)W.items.size();
+    if (W.n64 > 0)
+        ce.fn(false, dim3(W.grid), dim3(W.block), W.smem, s, d, W.d_items.p, W.n64, counters + ci);
+    if (n > W.n64)
+        ce.fn(true, dim3(W.grid32), dim3(W.block), W.smem, s, d, W.d_items.p + W.n64, n - W.n64,
+              counters + kNumClasses + ci);
+}
+
 static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s) {
     int st = ensure_pairs(c);
     if (st) return st;
@@ -1372,9 +1408,9 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         cutmat = c->d_cutmat.p;
     }
     QK_CUDA_TRY(c->d_A.reserve((size_t)n * n));
-    QK_CUDA_TRY(c->d_counters.reserve(kNumClasses));
+    QK_CUDA_TRY(c->d_counters.reserve(2 * kNumClasses));
     QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * n * n, s));
-    QK_CUDA_TRY(cudaMemsetAsync(c->d_counters.p, 0, sizeof(int) * kNumClasses, s));
+    QK_CUDA_TRY(cudaMemsetAsync(c->d_counters.p, 0, sizeof(int) * 2 * kNumClasses, s));
     DevData d = make_devdata(c);
     d.D = D;
     d.cutmat = cutmat;
@@ -1408,8 +1444,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         if (c->profile_stats) d.stats = c->d_stats.p + 2 * ci;
         if (c->profile_events) QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci], ls));
         const ClassEntry& ce = g_classes[ci];
-        ce.fn(dim3(W.grid), dim3(W.block), W.smem, ls, d, W.d_items.p,
-              (int)W.items.size(), c->d_counters.p + ci);
+        launch_class(ce, W, ls, d, c->d_counters.p, ci);
         QK_CUDA_TRY(cudaGetLastError());
         if (c->profile_events) {
             QK_CUDA_TRY(cudaEventRecord(c->ev[2 * ci + 1], ls));
@@ -1442,12 +1477,12 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
 // caller passes no density screen, that screen -- lives in this file-scope
 // array, which every GPU that loads the library holds until the process exits.
 // Layout in 8-byte words: [A: kNoAllocMaxNbasis^2][cutmat: kNoAllocMaxNshell^2]
-// [counters: kNumClasses ints].
+// [counters: 2 * kNumClasses ints].
 constexpr int kNoAllocMaxNbasis = 1024;
 constexpr int kNoAllocMaxNshell = 512;
 constexpr size_t kNoAllocWordsA = (size_t)kNoAllocMaxNbasis * kNoAllocMaxNbasis;
 constexpr size_t kNoAllocWordsCut = (size_t)kNoAllocMaxNshell * kNoAllocMaxNshell;
-constexpr size_t kNoAllocWords = kNoAllocWordsA + kNoAllocWordsCut + (kNumClasses + 1) / 2 + 1;
+constexpr size_t kNoAllocWords = kNoAllocWordsA + kNoAllocWordsCut + kNumClasses + 1;
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
 
 // Device address of g_noalloc_scratch, looked up once per device (in host code the
@@ -1502,7 +1537,7 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
     }
     // the array keeps the previous call's contents: clear what must start at zero
     QK_CUDA_TRY(cudaMemsetAsync(A, 0, sizeof(unsigned long long) * n * n, s));
-    QK_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * kNumClasses, s));
+    QK_CUDA_TRY(cudaMemsetAsync(counters, 0, sizeof(int) * 2 * kNumClasses, s));
     DevData d = make_devdata(c);
     d.D = D;
     d.cutmat = cutmat;
@@ -1520,8 +1555,7 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
             used[k] = true;
         }
         const ClassEntry& ce = g_classes[ci];
-        ce.fn(dim3(W.grid), dim3(W.block), W.smem, ls, d, W.d_items.p,
-              (int)W.items.size(), counters + ci);
+        launch_class(ce, W, ls, d, counters, ci);
         QK_CUDA_TRY(cudaGetLastError());
     }
     for (int k = 0; k < qk_ctx::kAux; ++k)
@@ -1548,7 +1582,7 @@ struct qk_batch {
     int device = 0;
     std::mutex mu;
     int num_sms = 148;
-    int bps[qk::kNumClasses] = {};            // resident blocks per SM of each batched class kernel
+    int bps[2 * qk::kNumClasses] = {};        // resident blocks per SM: FP64 kernels, then FP32 ones
     static constexpr int kStage = 2;
     char* h_stage[kStage] = {};
     size_t h_cap[kStage] = {};
@@ -1916,16 +1950,17 @@ qk_batch* qk_batch_create(int device, int* status) {
     for (int k = 0; ok && k < qk_batch::kAux; ++k)
         ok = cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming) == cudaSuccess;
-    for (int ci = 0; ok && ci < kNumClasses; ++ci) {
-        const ClassEntry& ce = g_classes[ci];
+    for (int slot = 0; ok && slot < 2 * kNumClasses; ++slot) {
+        const ClassEntry& ce = g_classes[slot % kNumClasses];
+        const bool fp32 = slot >= kNumClasses;
         const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
         if (ce.smem > 48 * 1024)
-            ok = cudaFuncSetAttribute(ce.kernel_batch(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ok = cudaFuncSetAttribute(ce.kernel_batch(fp32), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ce.smem) == cudaSuccess;
-        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->bps[ci], ce.kernel_batch(), 32 * wpb,
-                                                                 ce.smem) == cudaSuccess && b->bps[ci] >= 1;
+        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->bps[slot], ce.kernel_batch(fp32), 32 * wpb,
+                                                                 ce.smem) == cudaSuccess && b->bps[slot] >= 1;
     }
-    if (!ok || b->d_counters.reserve(kNumClasses) != cudaSuccess) {
+    if (!ok || b->d_counters.reserve(2 * kNumClasses) != cudaSuccess) {
         qk_batch_destroy(b);
         if (status) *status = fail(QK_ERR_CUDA, "qk_batch_create");
         return nullptr;
@@ -1979,21 +2014,30 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
         if (!(cutmat && cutmat[m])) QK_CUDA_TRY(c->d_cutmat.reserve((size_t)c->nshell * c->nshell));
         max_nn = std::max<long long>(max_nn, (long long)c->nbasis * c->nbasis);
     }
-    // staging block: [DevData x n][BatchMol x n][BatchSeg per class, classes in order]
-    int seg_count[kNumClasses], seg_off[kNumClasses], total_items[kNumClasses];
+    // staging block: [DevData x n][BatchMol x n][BatchSeg per slot]; slot ci = the
+    // FP64 items of class ci, slot kNumClasses + ci = its FP32 items (mixed form)
+    constexpr int kSlots = 2 * kNumClasses;
+    auto part_range = [&](const ClassWork& W, int slot, int* first, int* count) {
+        *first = slot < kNumClasses ? 0 : W.n64;
+        *count = slot < kNumClasses ? W.n64 : (int)W.items.size() - W.n64;
+    };
+    int seg_count[kSlots], seg_off[kSlots], total_items[kSlots];
     int nseg_all = 0;
-    for (int ci = 0; ci < kNumClasses; ++ci) {
-        seg_off[ci] = nseg_all;
-        seg_count[ci] = 0;
+    for (int slot = 0; slot < kSlots; ++slot) {
+        seg_off[slot] = nseg_all;
+        seg_count[slot] = 0;
         long long tot = 0;
-        for (int m = 0; m < n; ++m)
-            if (!ctxs[m]->work[ci].items.empty()) {
-                ++seg_count[ci];
-                tot += (long long)ctxs[m]->work[ci].items.size();
+        for (int m = 0; m < n; ++m) {
+            int f, cnt;
+            part_range(ctxs[m]->work[slot % kNumClasses], slot, &f, &cnt);
+            if (cnt > 0) {
+                ++seg_count[slot];
+                tot += cnt;
             }
+        }
         if (tot > INT_MAX) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: too many work items in one class");
-        total_items[ci] = (int)tot;
-        nseg_all += seg_count[ci];
+        total_items[slot] = (int)tot;
+        nseg_all += seg_count[slot];
     }
     const size_t off_mol = align16(sizeof(DevData) * n);
     const size_t off_seg = off_mol + align16(sizeof(BatchMol) * n);
@@ -2034,52 +2078,45 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
     const DevData* dd = (const DevData*)ds;
     const BatchMol* dm = (const BatchMol*)(ds + off_mol);
     const BatchSeg* dg = (const BatchSeg*)(ds + off_seg);
-    for (int ci = 0; ci < kNumClasses; ++ci) {
-        BatchSeg* sg = hg + seg_off[ci];
+    for (int slot = 0; slot < kSlots; ++slot) {
+        BatchSeg* sg = hg + seg_off[slot];
         int at = 0, ns = 0;
         for (int m = 0; m < n; ++m) {
-            const ClassWork& W = ctxs[m]->work[ci];
-            if (W.items.empty()) continue;
-            sg[ns++] = BatchSeg{W.d_items.p, at, m};
-            at += (int)W.items.size();
+            const ClassWork& W = ctxs[m]->work[slot % kNumClasses];
+            int f, cnt;
+            part_range(W, slot, &f, &cnt);
+            if (cnt <= 0) continue;
+            sg[ns++] = BatchSeg{W.d_items.p + f, at, m};
+            at += cnt;
         }
     }
     QK_CUDA_TRY(cudaMemcpyAsync(ds, hs, bytes, cudaMemcpyHostToDevice, s));
     QK_CUDA_TRY(cudaEventRecord(b->stage_ev[k], s));
-    QK_CUDA_TRY(cudaMemsetAsync(b->d_counters.p, 0, sizeof(int) * kNumClasses, s));
+    QK_CUDA_TRY(cudaMemsetAsync(b->d_counters.p, 0, sizeof(int) * kSlots, s));
     const int chunks = (int)std::min<long long>(64, std::max<long long>(1, (max_nn + 2047) / 2048));
     batch_prep_kernel<<<dim3(chunks, n), 256, 0, s>>>(dm);
     QK_CUDA_TRY(cudaGetLastError());
-    // class launches, cooperative (long) classes first, then by total items
-    int order[kNumClasses], no = 0;
-    for (int ci = 0; ci < kNumClasses; ++ci)
-        if (total_items[ci] > 0) order[no++] = ci;
+    // class launches one after another on the caller's stream (faster than
+    // concurrent launches that each fill the GPU), cooperative classes first
+    int order[kSlots], no = 0;
+    for (int slot = 0; slot < kSlots; ++slot)
+        if (total_items[slot] > 0) order[no++] = slot;
     std::stable_sort(order, order + no, [&](int x, int y) {
-        if (g_classes[x].coop != g_classes[y].coop) return g_classes[x].coop;
-        return (double)total_items[x] * g_classes[x].prim_flops > (double)total_items[y] * g_classes[y].prim_flops;
+        const ClassEntry& cx = g_classes[x % kNumClasses];
+        const ClassEntry& cy = g_classes[y % kNumClasses];
+        if (cx.coop != cy.coop) return cx.coop;
+        return (double)total_items[x] * cx.prim_flops > (double)total_items[y] * cy.prim_flops;
     });
-    QK_CUDA_TRY(cudaEventRecord(b->fork_ev, s));
-    bool used[qk_batch::kAux] = {};
     for (int i = 0; i < no; ++i) {
-        const int ci = order[i];
-        const ClassEntry& ce = g_classes[ci];
-        const int a = i % qk_batch::kAux;
-        if (!used[a]) {
-            QK_CUDA_TRY(cudaStreamWaitEvent(b->aux[a], b->fork_ev, 0));
-            used[a] = true;
-        }
+        const int slot = order[i];
+        const ClassEntry& ce = g_classes[slot % kNumClasses];
         const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
-        const long long need = ((long long)total_items[ci] + wpb - 1) / wpb;
-        const int grid = (int)std::min<long long>((long long)b->bps[ci] * b->num_sms, need);
-        ce.fn_batch(dim3(grid), dim3(32 * wpb), ce.smem, b->aux[a], dd, dg + seg_off[ci], seg_count[ci],
-                    total_items[ci], b->d_counters.p + ci);
+        const long long need = ((long long)total_items[slot] + wpb - 1) / wpb;
+        const int grid = (int)std::min<long long>((long long)b->bps[slot] * b->num_sms, need);
+        ce.fn_batch(slot >= kNumClasses, dim3(grid), dim3(32 * wpb), ce.smem, s, dd, dg + seg_off[slot],
+                    seg_count[slot], total_items[slot], b->d_counters.p + slot);
         QK_CUDA_TRY(cudaGetLastError());
     }
-    for (int a = 0; a < qk_batch::kAux; ++a)
-        if (used[a]) {
-            QK_CUDA_TRY(cudaEventRecord(b->join_ev[a], b->aux[a]));
-            QK_CUDA_TRY(cudaStreamWaitEvent(s, b->join_ev[a], 0));
-        }
     batch_finalize_kernel<<<dim3(chunks, n), 256, 0, s>>>(dm);
     QK_CUDA_TRY(cudaGetLastError());
     QK_CUDA_TRY(cudaEventRecord(b->done_ev, s));
