@@ -1012,7 +1012,6 @@ struct qk_ctx {
     int nstreams = 4;                 // class kernels run over this many streams (0: one after another)
     int cls_wpb[qk::kNumClasses] = {};    // warps per block of each class launch (0: default)
     int cls_bpsm[qk::kNumClasses] = {};   // cap on resident blocks per SM (0: as many as fit)
-    unsigned long long work_version = 0;   // bumped whenever the work lists are rebuilt
     double built_fp32 = -1.0;
     double built_cut = -1.0;
     bool pairs_dirty = true;
@@ -1092,13 +1091,6 @@ static double cons_expected(const int c[3]) {
         return std::sqrt(5.0) * std::sqrt(3.0);
     }
     return 1.0;
-}
-
-// Work-list versions are unique across all contexts of the process, so that a
-// batch never mistakes a new context at a freed context's address for the old one.
-static unsigned long long next_work_version() {
-    static std::atomic<unsigned long long> counter{0};
-    return ++counter;
 }
 
 static DevData make_devdata(qk_ctx* c) {
@@ -1347,7 +1339,6 @@ static int build_work(qk_ctx* c) {
         }
     }
     c->launches += 1;  // finalize
-    c->work_version = next_work_version();
     c->launch_order.clear();
     for (int ci = 0; ci < kNumClasses; ++ci)
         if (!c->work[ci].items.empty()) c->launch_order.push_back(ci);
@@ -1576,8 +1567,8 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
 // -- the molecules' DevData, their BatchMol records and every class's segment
 // table -- into pinned memory (two blocks, used in turn, each guarded by the
 // event of its last copy), copies it to the device with one cudaMemcpyAsync, and
-// enqueues: counters memset, batch_prep_kernel, the class kernels (forked over
-// auxiliary streams), batch_finalize_kernel.
+// enqueues on the caller's stream: counters memset, batch_prep_kernel, the class
+// kernels (FP64 and FP32 parts, one after another), batch_finalize_kernel.
 struct qk_batch {
     int device = 0;
     std::mutex mu;
@@ -1592,9 +1583,6 @@ struct qk_batch {
     qk::DevBuf<int> d_counters;
     cudaEvent_t done_ev = nullptr;            // end of the previous build (orders reuse of d_stage)
     bool done_recorded = false;
-    static constexpr int kAux = 4;
-    cudaStream_t aux[kAux] = {};
-    cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
 };
 
 using namespace qk;
@@ -1943,13 +1931,9 @@ qk_batch* qk_batch_create(int device, int* status) {
     qk_batch* b = new qk_batch();
     b->device = device;
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
-    bool ok = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&b->done_ev, cudaEventDisableTiming) == cudaSuccess;
+    bool ok = cudaEventCreateWithFlags(&b->done_ev, cudaEventDisableTiming) == cudaSuccess;
     for (int k = 0; ok && k < qk_batch::kStage; ++k)
         ok = cudaEventCreateWithFlags(&b->stage_ev[k], cudaEventDisableTiming) == cudaSuccess;
-    for (int k = 0; ok && k < qk_batch::kAux; ++k)
-        ok = cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming) == cudaSuccess;
     for (int slot = 0; ok && slot < 2 * kNumClasses; ++slot) {
         const ClassEntry& ce = g_classes[slot % kNumClasses];
         const bool fp32 = slot >= kNumClasses;
@@ -1973,15 +1957,10 @@ int qk_batch_destroy(qk_batch* b) {
     if (!b) return QK_OK;
     cudaSetDevice(b->device);
     cudaDeviceSynchronize();
-    for (auto& a : b->aux)
-        if (a) cudaStreamDestroy(a);
-    for (auto& e : b->join_ev)
-        if (e) cudaEventDestroy(e);
     for (int k = 0; k < qk_batch::kStage; ++k) {
         if (b->stage_ev[k]) cudaEventDestroy(b->stage_ev[k]);
         if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
     }
-    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
     if (b->done_ev) cudaEventDestroy(b->done_ev);
     delete b;
     return QK_OK;
