@@ -178,6 +178,10 @@ qk_batch *qk_batch_create(int device, int *status);
 int qk_batch_destroy(qk_batch *batch);
 int qk_batch_fock2e(qk_batch *batch, int n, qk_ctx *const *ctx, const double *const *D_dev,
                     const double *const *cutmat_dev, double *const *o_dev, void *stream);
+/* Size the batch's persistent class kernels for all SMs but `sms` (default 0), so
+ * that other work on the GPU -- e.g. the set-up of new molecules on other streams
+ * -- finds free SMs while a batch runs.  Same results. */
+int qk_batch_reserve_sms(qk_batch *batch, int sms);
 
 /* Work statistics of the last build: shell quartets listed and primitive quartets
  * listed after Schwarz screening (before density screening). */

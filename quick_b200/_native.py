@@ -24,7 +24,7 @@ EXPORTED = [
     "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc", "qk_set_precision",
     "qk_last_work_mixed", "qk_batch_create", "qk_batch_destroy", "qk_batch_fock2e",
     "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_set_streams",
-    "qk_set_class_launch", "qk_class_launch",
+    "qk_set_class_launch", "qk_class_launch", "qk_batch_reserve_sms",
 ]
 
 _lib = None
@@ -79,6 +79,7 @@ def lib():
     L.qk_batch_create.argtypes = [I, PI]
     L.qk_batch_destroy.argtypes = [P]
     L.qk_batch_fock2e.argtypes = [P, I, P, P, P, P, P]
+    L.qk_batch_reserve_sms.argtypes = [P, I]
     L.qk_prepare.argtypes = [P]
     L.qk_set_streams.argtypes = [P, I]
     L.qk_set_class_launch.argtypes = [P, I, I, I]

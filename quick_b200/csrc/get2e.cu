@@ -1583,6 +1583,7 @@ struct qk_batch {
     qk::DevBuf<int> d_counters;
     cudaEvent_t done_ev = nullptr;            // end of the previous build (orders reuse of d_stage)
     bool done_recorded = false;
+    int reserve_sms = 0;                      // SMs the class kernels leave to other work
 };
 
 using namespace qk;
@@ -1970,6 +1971,13 @@ namespace {
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 }
 
+int qk_batch_reserve_sms(qk_batch* b, int sms) {
+    if (!b || sms < 0) return fail(QK_ERR_INVALID_ARG, "qk_batch_reserve_sms");
+    std::lock_guard<std::mutex> g(b->mu);
+    b->reserve_sms = std::min(sms, b->num_sms - 1);
+    return QK_OK;
+}
+
 int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const* D, const double* const* cutmat,
                     double* const* o, void* stream) {
     if (!b || n <= 0 || !ctxs || !D || !o) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: null argument");
@@ -2091,7 +2099,8 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
         const ClassEntry& ce = g_classes[slot % kNumClasses];
         const int wpb = ce.coop ? ce.coop_warps : kWarpsPerBlock;
         const long long need = ((long long)total_items[slot] + wpb - 1) / wpb;
-        const int grid = (int)std::min<long long>((long long)b->bps[slot] * b->num_sms, need);
+        const int sms = std::max(1, b->num_sms - b->reserve_sms);
+        const int grid = (int)std::min<long long>((long long)b->bps[slot] * sms, need);
         ce.fn_batch(slot >= kNumClasses, dim3(grid), dim3(32 * wpb), ce.smem, s, dd, dg + seg_off[slot],
                     seg_count[slot], total_items[slot], b->d_counters.p + slot);
         QK_CUDA_TRY(cudaGetLastError());

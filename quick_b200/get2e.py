@@ -202,6 +202,10 @@ class Get2eBatch:
         except Exception:
             pass
 
+    def reserve_sms(self, sms: int):
+        """Leave ``sms`` SMs free of the batch's class kernels (for concurrent work)."""
+        check(lib().qk_batch_reserve_sms(self.h, int(sms)), "qk_batch_reserve_sms")
+
     def fock2e(self, engines, Ds, os=None, cutmats=None, stream=None):
         """o[m] += G(D[m]) for every engine m; tensors are CUDA float64.
 
