@@ -236,7 +236,7 @@ class Server:
     def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
                  denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
                  max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64,
-                 workers: int = 4, scf: str = "device", reserve_sms: int = 8):
+                 workers: int = 4, scf: str = "device", reserve_sms: int = 0):
         import torch
         from .get2e import Get2eBatch
         self.torch = torch
@@ -255,10 +255,9 @@ class Server:
         self.pool = []                # (Get2e, bytes) kept for reuse
         self._arrival = lambda r: r.arrival
         self.batch = Get2eBatch(device)
-        if workers > 0:
-            # the set-up threads' kernels (Schwarz bounds, one-electron integrals,
-            # guess) find free SMs while a batch's persistent kernels run
-            self.batch.reserve_sms(reserve_sms)
+        # reserve_sms > 0 leaves SMs to the set-up threads' kernels while a batch's
+        # persistent kernels run (measured: no gain beyond the run-to-run spread)
+        self.batch.reserve_sms(reserve_sms)
         self.active = []
         self.queue = deque()
         self.series_D = {}            # series -> last converged density (device)
