@@ -557,8 +557,14 @@ def main(argv=None):
     ap.add_argument("--budget-gb", type=float, default=None)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--warmup", type=int, default=64,
+                    help="requests served (untimed) first: module loading, SAD atoms, allocator")
     a = ap.parse_args(argv)
     budget = int(a.budget_gb * (1 << 30)) if a.budget_gb else None
+    if a.warmup > 0:
+        w = Server(memory_budget=budget)
+        w.serve(request_stream(a.warmup, 1000.0, seed=a.seed + 1), realtime=False)
+        w.close()
     report = []
     for rate in a.rate:
         if a.compare:
