@@ -377,6 +377,15 @@ __device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp
     }
 }
 
+// Asynchronous global -> shared copies (cp.async, 8 bytes), used to bring a
+// quartet's density blocks in while its VRR runs.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <int La, int Lb, int Lc, int Ld>
 __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, double* acc, double* V, double* Db,
                                              int lane, int* nq_done, int* np_done) {
@@ -400,6 +409,22 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     const double Cx = d.xyz[3 * ic], Cy = d.xyz[3 * ic + 1], Cz = d.xyz[3 * ic + 2];
     const double CDx = Cx - d.xyz[3 * id], CDy = Cy - d.xyz[3 * id + 1], CDz = Cz - d.xyz[3 * id + 2];
 
+    // the six density blocks, copied into shared memory while the VRR runs
+    const int fa = d.q_f0[qa], fb = d.q_f0[qb], fc = d.q_f0[qc], fd = d.q_f0[qd];
+    double* Dab = Db;
+    double* Dcd = Dab + NAB;
+    double* Dbd = Dcd + NCD;
+    double* Dad = Dbd + NB * ND;
+    double* Dbc = Dad + NA * ND;
+    double* Dac = Dbc + NB * NC;
+    for (int t = lane; t < NAB; t += 32) cp_async8(Dab + t, d.D + (size_t)(fa + t / NB) * n + fb + t % NB);
+    for (int t = lane; t < NCD; t += 32) cp_async8(Dcd + t, d.D + (size_t)(fc + t / ND) * n + fd + t % ND);
+    for (int t = lane; t < NB * ND; t += 32) cp_async8(Dbd + t, d.D + (size_t)(fb + t / ND) * n + fd + t % ND);
+    for (int t = lane; t < NA * ND; t += 32) cp_async8(Dad + t, d.D + (size_t)(fa + t / ND) * n + fd + t % ND);
+    for (int t = lane; t < NB * NC; t += 32) cp_async8(Dbc + t, d.D + (size_t)(fb + t / NC) * n + fc + t % NC);
+    for (int t = lane; t < NA * NC; t += 32) cp_async8(Dac + t, d.D + (size_t)(fa + t / NC) * n + fc + t % NC);
+    cp_async_commit();
+
     coop_contract<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q], d.pr_pps[Q],
                                   Cx, Cy, Cz, dnmax, true, acc, V, lane, np_done);
     __syncwarp();   // acc complete (also when every primitive quartet was screened out)
@@ -408,26 +433,14 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     double* I = V + NF * NAB;
     for (int f = lane; f < NF; f += 32) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, ABx, ABy, ABz);
     __syncwarp();
-    for (int ab = lane; ab < NAB; ab += 32) Cls::hrr_ket(t1 + ab, NAB, I + ab * NCD, CDx, CDy, CDz);
-    // density blocks
-    const int fa = d.q_f0[qa], fb = d.q_f0[qb], fc = d.q_f0[qc], fd = d.q_f0[qd];
-    double* Dab = Db;
-    double* Dcd = Dab + NAB;
-    double* Dbd = Dcd + NCD;
-    double* Dad = Dbd + NB * ND;
-    double* Dbc = Dad + NA * ND;
-    double* Dac = Dbc + NB * NC;
-    for (int t = lane; t < NAB; t += 32) Dab[t] = d.D[(fa + t / NB) * n + fb + t % NB];
-    for (int t = lane; t < NCD; t += 32) Dcd[t] = d.D[(fc + t / ND) * n + fd + t % ND];
-    for (int t = lane; t < NB * ND; t += 32) Dbd[t] = d.D[(fb + t / ND) * n + fd + t % ND];
-    for (int t = lane; t < NA * ND; t += 32) Dad[t] = d.D[(fa + t / ND) * n + fd + t % ND];
-    for (int t = lane; t < NB * NC; t += 32) Dbc[t] = d.D[(fb + t / NC) * n + fc + t % NC];
-    for (int t = lane; t < NA * NC; t += 32) Dac[t] = d.D[(fa + t / NC) * n + fc + t % NC];
-    __syncwarp();
-    for (int t = lane; t < NAB * NCD; t += 32) {
-        const int ab = t / NCD, cd = t % NCD;
-        I[t] *= Cls::cons_a(ab / NB) * Cls::cons_b(ab % NB) * Cls::cons_c(cd / ND) * Cls::cons_d(cd % ND);
+    // ket HRR one bra row per lane, the row scaled by QUICK's cons factors as it is written
+    for (int ab = lane; ab < NAB; ab += 32) {
+        double* row = I + ab * NCD;
+        Cls::hrr_ket(t1 + ab, NAB, row, CDx, CDy, CDz);
+        const double cab = Cls::cons_a(ab / NB) * Cls::cons_b(ab % NB);
+        for (int cd = 0; cd < NCD; ++cd) row[cd] *= cab * Cls::cons_c(cd / ND) * Cls::cons_d(cd % ND);
     }
+    cp_async_wait_all();
     __syncwarp();
     const double deg = (qa != qb ? 2.0 : 1.0) * (qc != qd ? 2.0 : 1.0) * (P != Q ? 2.0 : 1.0);
     const double wJ = 0.25 * deg, wK = -0.0625 * deg;
