@@ -116,7 +116,12 @@ int qk_set_basis(qk_ctx *ctx, int natom, const double *xyz, int nshell, int nbas
 int qk_schwarz(qk_ctx *ctx, double *YCutoff, double *cutPrim);
 /* Install caller-provided Schwarz bounds (same layout as gpu_upload_cutoff_matrix_). */
 int qk_set_schwarz(qk_ctx *ctx, const double *YCutoff, const double *cutPrim);
-/* integralCutoff and primLimit (src/modules/quick_method_module.f90:772-775). */
+/* integralCutoff and primLimit (src/modules/quick_method_module.f90:772-775).  Every
+ * build applies the cutoffs in force (the CPU get2e's tests Y_ij*Y_kl > cut and
+ * Y_ij*Y_kl*DNmax > cut).  The work lists are rebuilt only when the cutoff tightens
+ * below the one they were built at: an SCF that tightens its cutoff as it converges
+ * (adjust_Cutoff, src/modules/quick_method_module.f90:1107-1129) sets the final cutoff,
+ * calls qk_prepare, then loosens it, and the lists are built once. */
 int qk_set_cutoffs(qk_ctx *ctx, double integralCutoff, double primLimit);
 /* Mixed precision (no counterpart in the reference, which is FP64 throughout): quartets
  * whose Schwarz bound product Y_ij*Y_kl is below fp32_bound evaluate the vertical
@@ -131,8 +136,9 @@ int qk_last_work_mixed(qk_ctx *ctx, long long *quartets_fp32);
  * density screen (max |D| per shell pair) or NULL to derive it from D_dev on the device
  * (cshell_density_cutoff, src/modules/include/cutoff.fh:62-92).  Enqueued on `stream`
  * (a cudaStream_t; NULL = the CUDA default stream); returns without synchronising.
- * The first call after a basis, Schwarz or cutoff change also builds the pair tables
- * and work lists on the host and waits for their upload. */
+ * The first call after a basis or Schwarz change, or after the cutoff tightens below
+ * the one the lists were built at, also builds the pair tables and work lists on the
+ * host and waits for their upload. */
 int qk_fock2e_device(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
                      double *o_dev, void *stream);
 /* Same with host buffers (copies D in, adds G into o, synchronises). */
@@ -149,8 +155,8 @@ int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_de
  * cutmat_dev is NULL, the density screen) lives in one array inside the library that
  * every GPU loading it holds until exit: limits nbasis <= 1024 and, with
  * cutmat_dev == NULL, nshell <= 512; larger sizes return QK_ERR_INVALID_ARG.
- * The pair tables must already exist: run qk_fock2e_device once after any basis,
- * Schwarz or cutoff change, else QK_ERR_NOT_READY.  The first call on a device looks
+ * The pair tables must already exist: run qk_fock2e_device (or qk_prepare) once after
+ * any basis or Schwarz change or a tightening of the cutoff, else QK_ERR_NOT_READY.  The first call on a device looks
  * up the array's device address; make it before any stream capture.  All calls share
  * the array, so calls that overlap on the GPU race: keep them on one stream (or order
  * them with events). */

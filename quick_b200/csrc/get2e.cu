@@ -164,7 +164,9 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
     dnmax = fmax(dnmax, fmax(cm[sa * ns + sd], cm[sa * ns + sc]));
     dnmax = fmax(dnmax, fmax(cm[sb * ns + sc], cm[sb * ns + sd]));
     const double ct = d.pr_Y[P] * d.pr_Y[Q];
-    if (!(ct * dnmax > d.cut)) return;
+    // the CPU get2e's two tests (Y_P Y_Q > cut, then with DNmax): the work list may
+    // have been built at a tighter cutoff than the one in force
+    if (!(ct > d.cut) || !(ct * dnmax > d.cut)) return;
     ++*nq_done;
 
     const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
@@ -401,7 +403,7 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     dnmax = fmax(dnmax, fmax(cm[sa * ns + sd], cm[sa * ns + sc]));
     dnmax = fmax(dnmax, fmax(cm[sb * ns + sc], cm[sb * ns + sd]));
     const double ct = d.pr_Y[P] * d.pr_Y[Q];
-    if (!(ct * dnmax > d.cut)) return;            // warp-uniform
+    if (!(ct > d.cut) || !(ct * dnmax > d.cut)) return;   // warp-uniform
     if (lane == 0) ++*nq_done;
     const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
     const double ABx = d.xyz[3 * ia] - d.xyz[3 * ib], ABy = d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
@@ -1374,7 +1376,11 @@ static int build_work(qk_ctx* c) {
 static int ensure_pairs(qk_ctx* c) {
     if (!c->have_basis) return fail(QK_ERR_NOT_READY, "basis not uploaded");
     if (!c->have_schwarz) return fail(QK_ERR_NOT_READY, "Schwarz bounds not set");
-    if (!c->pairs_dirty && c->built_cut == c->integralCutoff && c->built_fp32 == c->fp32_bound) return QK_OK;
+    // Lists built at a tighter cutoff than the one in force are kept: they hold
+    // every quartet the looser cutoff admits, and the kernels apply the cutoff in
+    // force themselves (an SCF that tightens its cutoff as it converges builds
+    // its lists once, at the final cutoff).
+    if (!c->pairs_dirty && c->built_cut <= c->integralCutoff && c->built_fp32 == c->fp32_bound) return QK_OK;
     build_pairs(c, true);
     int st = upload_pairs(c);
     if (st) return st;
@@ -1522,7 +1528,7 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
         return fail(QK_ERR_INVALID_ARG,
                     "qk_fock2e_device_noalloc: nshell exceeds the fixed density-screen scratch (max 512); "
                     "pass cutmat_dev");
-    if (!c->have_basis || !c->have_schwarz || c->pairs_dirty || c->built_cut != c->integralCutoff)
+    if (!c->have_basis || !c->have_schwarz || c->pairs_dirty || c->built_cut > c->integralCutoff)
         return fail(QK_ERR_NOT_READY,
                     "qk_fock2e_device_noalloc: pair tables not built for the current basis/Schwarz/cutoffs; "
                     "run qk_fock2e_device once first");

@@ -37,6 +37,66 @@ from .get2e import Get2e
 # below 0.2, which is then opened to 0.2.
 LSHIFT_CYCLE, LSHIFT_ERR, LSHIFT_GAP = 3, 0.1, 0.2
 
+# The tightest integral cutoff QUICK's SCF schedule reaches (adjust_Cutoff below).
+FINAL_CUTOFF = 1e-11
+
+
+def adjust_cutoff(prms: float, cut: float, prim: float):
+    """QUICK's integral cutoff during the SCF (``adjust_Cutoff``,
+    ``src/modules/quick_method_module.f90:1107-1129``, called after every cycle
+    with the RMS density change, ``quick_scf_module.f90:679-680``): once PRMS is
+    at or below 1e-5, 1e-6, 1e-7 the cutoff tightens to 1e-9, 1e-10, 1e-11 --
+    each step only from a cutoff looser than 10^-8.5, 10^-9.5, 10^-10.5 -- and
+    primLimit follows it down.  The three tests run in turn, so one call may take
+    several steps.  Returns (integral cutoff, primLimit)."""
+    for p, above, new in ((1e-5, 10.0 ** -8.5, 1e-9), (1e-6, 10.0 ** -9.5, 1e-10), (1e-7, 10.0 ** -10.5, 1e-11)):
+        if prms <= p and cut > above:
+            cut = new
+            prim = min(cut, prim)
+    return cut, prim
+
+
+class CutoffSchedule:
+    """The cutoffs of one solve on its engine.  Disabled: the engine's cutoffs
+    hold throughout.  Enabled: the solve starts at the engine's cutoffs and
+    tightens them by :func:`adjust_cutoff` after every cycle; the work lists are
+    built once, at the final cutoff, before the first build (the builds apply the
+    cutoff in force themselves, so the lists only have to hold every quartet it
+    admits), and :meth:`restore` puts the starting cutoffs back.  As in QUICK the
+    incremental builds carry on across a change (no full rebuild)."""
+
+    def __init__(self, eng, enabled: bool):
+        self.eng, self.enabled = eng, bool(enabled)
+        self.start = (eng.integral_cutoff, eng.prim_limit)
+        self.cut, self.prim = self.start
+        self.changes = []
+        if self.enabled:
+            final = min(self.cut, FINAL_CUTOFF)
+            if final < self.cut:
+                eng.set_cutoffs(final, self.prim)
+                eng.prepare()
+                eng.set_cutoffs(self.cut, self.prim)
+
+    def update(self, it: int, prms: float) -> bool:
+        """Apply the schedule after cycle ``it``; True when the cutoffs changed."""
+        if not self.enabled:
+            return False
+        cut, prim = adjust_cutoff(prms, self.cut, self.prim)
+        if (cut, prim) == (self.cut, self.prim):
+            return False
+        self.cut, self.prim = cut, prim
+        self.eng.set_cutoffs(cut, prim)
+        self.changes.append((it, cut, prim))
+        return True
+
+    def restore(self) -> bool:
+        """Put the starting cutoffs back; True when they had changed."""
+        if self.enabled and (self.cut, self.prim) != self.start:
+            self.eng.set_cutoffs(*self.start)
+            self.cut, self.prim = self.start
+            return True
+        return False
+
 
 def oei(basis, ext_charges=None, device=0):
     """S, T, V (nbasis^2 numpy) computed on the GPU."""
@@ -116,14 +176,15 @@ class RHF:
         return self.density(F0)
 
     def state(self, denserms: float = 1e-6, maxiter: int = 100, guess="sad", incremental: bool = True,
-              ncyc: int = 3, maxdiis: int = 10, D0=None):
-        """A solve that advances one Fock build at a time (:class:`SCFState`)."""
-        return SCFState(self, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0)
+              ncyc: int = 3, maxdiis: int = 10, D0=None, adaptive_cutoff: bool = False):
+        """A solve that advances one Fock build at a time (:class:`SCFState`).
+        ``adaptive_cutoff``: QUICK's cutoff schedule (:class:`CutoffSchedule`)."""
+        return SCFState(self, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0, adaptive_cutoff)
 
     def run(self, denserms: float = 1e-6, maxiter: int = 100, guess="sad", incremental: bool = True,
-            ncyc: int = 3, maxdiis: int = 10, D0=None, verbose=False):
+            ncyc: int = 3, maxdiis: int = 10, D0=None, verbose=False, adaptive_cutoff: bool = False):
         t0 = time.perf_counter()
-        st = self.state(denserms, maxiter, guess, incremental, ncyc, maxdiis, D0)
+        st = self.state(denserms, maxiter, guess, incremental, ncyc, maxdiis, D0, adaptive_cutoff)
         while not st.done:
             Db, F = st.fock_input()
             self.eng.fock2e(Db, o=F)
@@ -157,8 +218,9 @@ class SCFState:
        cycles).
     """
 
-    def __init__(self, rhf, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0):
+    def __init__(self, rhf, denserms, maxiter, guess, incremental, ncyc, maxdiis, D0, adaptive_cutoff=False):
         self.rhf = rhf
+        self.cutoffs = CutoffSchedule(rhf.eng, adaptive_cutoff)
         self.torch = rhf.torch
         self.denserms, self.maxiter = denserms, maxiter
         self.incremental, self.ncyc, self.maxdiis = incremental, ncyc, maxdiis
@@ -242,11 +304,14 @@ class SCFState:
             self.D = self.Dn
         else:
             self.D = self.Dn
+            self.cutoffs.update(self.it, prms)
 
     def result(self):
         r = self.rhf
+        self.cutoffs.restore()
         return {"E": self.Eel + r.Ecore, "Eel": self.Eel, "Ecore": r.Ecore, "D": self.D, "F": self.F,
-                "niter": self.it, "converged": self.converged, "history": self.history}
+                "niter": self.it, "converged": self.converged, "history": self.history,
+                "cutoff_changes": list(self.cutoffs.changes)}
 
 
 def gershgorin_range(Fo) -> float:
@@ -428,11 +493,13 @@ class GraphSCF:
         self.focks.zero_()
 
     def run(self, denserms: float = 1e-6, maxiter: int = 100, guess: str = "sad", ncyc: int = 3, D0=None,
-            graph: bool = True):
+            graph: bool = True, adaptive_cutoff: bool = False):
         torch = self.torch
         r = self.rhf
         t0 = time.perf_counter()
-        st = DeviceSCFState(r, denserms=denserms, maxiter=maxiter, guess=guess, ncyc=ncyc, D0=D0, g=self)
+        st = DeviceSCFState(r, denserms=denserms, maxiter=maxiter, guess=guess, ncyc=ncyc, D0=D0, g=self,
+                            adaptive_cutoff=adaptive_cutoff)
+        replayed = False
         while not st.done:
             if graph and st.it + 1 >= ncyc:
                 st.it += 1
@@ -442,6 +509,7 @@ class GraphSCF:
                     with torch.cuda.graph(self.graph):
                         self._body()
                 self.graph.replay()
+                replayed = True
             else:
                 dD, F = st.fock_input()
                 r.eng.fock2e(dD, o=F)
@@ -449,7 +517,7 @@ class GraphSCF:
             st.step(self.out.cpu().numpy())
         torch.cuda.synchronize(r.device)
         res = st.result()
-        res.update({"seconds": time.perf_counter() - t0, "sp2_steps": self.sp2, "graph": self.graph is not None,
+        res.update({"seconds": time.perf_counter() - t0, "sp2_steps": self.sp2, "graph": replayed,
                     "recaptures": self.recaptures})
         return res
 
@@ -466,8 +534,9 @@ class DeviceSCFState:
     _pools = {}
 
     def __init__(self, rhf, denserms=1e-6, maxiter=100, guess="sad", ncyc=3, D0=None, maxdiis=10, g=None,
-                 graph: bool = False):
+                 graph: bool = False, adaptive_cutoff: bool = False):
         self.rhf = rhf
+        self.cutoffs = CutoffSchedule(rhf.eng, adaptive_cutoff)
         self.g = g if g is not None else GraphSCF(rhf, maxdiis=maxdiis)
         # graph=True: the post-build half of a cycle is captured once and replayed
         # (one launch per solve and step instead of some hundred)
@@ -546,9 +615,15 @@ class DeviceSCFState:
             self.converged = self.done = True
         elif self.it >= self.maxiter:
             self.done = True
+        elif self.cutoffs.update(self.it, prms):
+            g.graph = None              # a captured build holds the cutoffs it was captured with
+            g.recaptures += 1
 
     def result(self):
         g, r = self.g, self.rhf
+        if self.cutoffs.restore():
+            g.graph = None
         D = g.Dref.clone() if self.converged else g.D.clone()
         return {"E": self.Eel + r.Ecore, "Eel": self.Eel, "Ecore": r.Ecore, "D": D, "F": g.F.clone(),
-                "niter": self.it, "converged": self.converged, "history": self.history}
+                "niter": self.it, "converged": self.converged, "history": self.history,
+                "cutoff_changes": list(self.cutoffs.changes)}
