@@ -209,6 +209,14 @@ def best_hrr(La, Lb):
 
 
 COOP_MIN = 150   # NE*NF at or above which a class uses the warp-cooperative kernel
+# f classes evaluated per lane although the f rule in is_coop would make them
+# cooperative: their per-lane kernels keep almost all of their state in registers
+# (0.1-5 KB local frames under -Xptxas -v) and ran 1.4-5.6x faster than the
+# cooperative kernel on B200 (per-class CUDA-event times, 12 H2O / cc-pVTZ).  The
+# other classes above the rules were measured per lane too and spill 15-27 KB per
+# lane (dpdp, ddpp, ddds, ddfs, fppp, fpfs, fdds): 3-6x slower than cooperative.
+PER_LANE = {(3, 0, 1, 1), (3, 0, 2, 0), (3, 0, 2, 1), (3, 0, 3, 0), (3, 1, 1, 0), (3, 1, 2, 0),
+            (3, 2, 1, 0), (3, 3, 0, 0), (3, 3, 1, 0)}
 SMEM_MAX = 227 * 1024   # shared memory of one block
 
 
@@ -218,6 +226,8 @@ def is_coop(La, Lb, Lc, Ld):
     NE = sum(ncart(L) for L in range(La, Lab + 1))
     NF = sum(ncart(L) for L in range(Lc, Lcd + 1))
     nint = ncart(La) * ncart(Lb) * ncart(Lc) * ncart(Ld)
+    if (La, Lb, Lc, Ld) in PER_LANE:
+        return False
     if max(La, Lb, Lc, Ld) >= 3:
         return NE * NF >= 60 or nint > 60
     return NE * NF >= COOP_MIN
