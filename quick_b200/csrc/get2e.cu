@@ -388,6 +388,48 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Digestion of one quartet by the warp, one group of outputs at a time (J_ab,
+// J_cd, K_ac, K_bc, K_ad, K_bd).  A group has NOUT outputs, each a dot product
+// over the terms (k1, k2), k1 < N1, k2 < N2, of the integral I[base(o) + k1*ST1 +
+// k2*ST2] and the density element Dv[k1*N2 + k2].  S lanes share an output (S a
+// power of two <= N1, fixed per group at compile time): each takes every S-th k1
+// and all k2, and the partial sums meet in a fixed shuffle tree, so the sums do
+// not depend on timing.  S minimises rounds x (terms per lane + shuffle steps +
+// the round's address and atomic work):
+// groups with few outputs and long sums (J_cd, K_ad, K_bd of the d classes) no
+// longer run on a handful of lanes while the others wait.
+__host__ __device__ constexpr int digest_cost(int nout, int n1, int n2, int s) {
+    int lg = 0;
+    for (int t = s; t > 1; t >>= 1) ++lg;
+    return ((nout * s + 31) / 32) * (((n1 + s - 1) / s) * n2 + 4 * lg + 8);   // + 8: a round's own work
+}
+__host__ __device__ constexpr int digest_split(int nout, int n1, int n2) {
+    int best = 1;
+    for (int s = 2; s <= 32; s *= 2)
+        if (s <= n1 && digest_cost(nout, n1, n2, s) < digest_cost(nout, n1, n2, best)) best = s;
+    return best;
+}
+template <int NOUT, int N1, int N2, int ST1, int ST2, typename Base, typename Addr>
+__device__ __forceinline__ void digest_group(int lane, double w, unsigned long long* A, const double* I,
+                                             const double* Dv, Base base, Addr addr) {
+    constexpr int S = digest_split(NOUT, N1, N2);
+    constexpr int PER = 32 / S;   // outputs per round
+    for (int o0 = 0; o0 < NOUT; o0 += PER) {
+        const int o = o0 + lane / S, p = lane % S;
+        double sum = 0.0;
+        if (o < NOUT) {
+            const double* row = I + base(o);
+            for (int k1 = p; k1 < N1; k1 += S) {
+#pragma unroll
+                for (int k2 = 0; k2 < N2; ++k2) sum = fma(row[k1 * ST1 + k2 * ST2], Dv[k1 * N2 + k2], sum);
+            }
+        }
+#pragma unroll
+        for (int off = S / 2; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, S);
+        if (o < NOUT && p == 0) atomic_fixed(A + addr(o), w * sum);
+    }
+}
+
 template <int La, int Lb, int Lc, int Ld>
 __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, double* acc, double* V, double* Db,
                                              int lane, int* nq_done, int* np_done) {
@@ -446,43 +488,27 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     __syncwarp();
     const double deg = (qa != qb ? 2.0 : 1.0) * (qc != qd ? 2.0 : 1.0) * (P != Q ? 2.0 : 1.0);
     const double wJ = 0.25 * deg, wK = -0.0625 * deg;
-    constexpr int O1 = NAB, O2 = O1 + NCD, O3 = O2 + NA * NC, O4 = O3 + NB * NC, O5 = O4 + NA * ND,
-                  O6 = O5 + NB * ND;
     unsigned long long* A = d.A;
-    for (int t = lane; t < O6; t += 32) {
-        double sum = 0.0;
-        size_t addr;
-        double w;
-        if (t < O1) {                 // J over the bra: (ab) row . Dcd
-            for (int cd = 0; cd < NCD; ++cd) sum = fma(I[t * NCD + cd], Dcd[cd], sum);
-            addr = (size_t)(fa + t / NB) * n + fb + t % NB; w = wJ;
-        } else if (t < O2) {          // J over the ket
-            const int cd = t - O1;
-            for (int ab = 0; ab < NAB; ++ab) sum = fma(I[ab * NCD + cd], Dab[ab], sum);
-            addr = (size_t)(fc + cd / ND) * n + fd + cd % ND; w = wJ;
-        } else if (t < O3) {          // K_ac = sum_bd I D_bd
-            const int a = (t - O2) / NC, c = (t - O2) % NC;
-            for (int b = 0; b < NB; ++b)
-                for (int e = 0; e < ND; ++e) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dbd[b * ND + e], sum);
-            addr = (size_t)(fa + a) * n + fc + c; w = wK;
-        } else if (t < O4) {          // K_bc = sum_ad I D_ad
-            const int b = (t - O3) / NC, c = (t - O3) % NC;
-            for (int a = 0; a < NA; ++a)
-                for (int e = 0; e < ND; ++e) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dad[a * ND + e], sum);
-            addr = (size_t)(fb + b) * n + fc + c; w = wK;
-        } else if (t < O5) {          // K_ad = sum_bc I D_bc
-            const int a = (t - O4) / ND, e = (t - O4) % ND;
-            for (int b = 0; b < NB; ++b)
-                for (int c = 0; c < NC; ++c) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dbc[b * NC + c], sum);
-            addr = (size_t)(fa + a) * n + fd + e; w = wK;
-        } else {                      // K_bd = sum_ac I D_ac
-            const int b = (t - O5) / ND, e = (t - O5) % ND;
-            for (int a = 0; a < NA; ++a)
-                for (int c = 0; c < NC; ++c) sum = fma(I[(a * NB + b) * NCD + c * ND + e], Dac[a * NC + c], sum);
-            addr = (size_t)(fb + b) * n + fd + e; w = wK;
-        }
-        atomic_fixed(A + addr, w * sum);
-    }
+    // J over the bra: (ab) row . Dcd;  J over the ket: (cd) column . Dab
+    digest_group<NAB, NC, ND, ND, 1>(
+        lane, wJ, A, I, Dcd, [&](int ab) { return ab * NCD; },
+        [&](int ab) { return (size_t)(fa + ab / NB) * n + fb + ab % NB; });
+    digest_group<NCD, NA, NB, NB * NCD, NCD>(
+        lane, wJ, A, I, Dab, [&](int cd) { return cd; },
+        [&](int cd) { return (size_t)(fc + cd / ND) * n + fd + cd % ND; });
+    // K_ac = sum_bd I D_bd,  K_bc = sum_ad I D_ad,  K_ad = sum_bc I D_bc,  K_bd = sum_ac I D_ac
+    digest_group<NA * NC, NB, ND, NCD, 1>(
+        lane, wK, A, I, Dbd, [&](int ac) { return (ac / NC) * NB * NCD + (ac % NC) * ND; },
+        [&](int ac) { return (size_t)(fa + ac / NC) * n + fc + ac % NC; });
+    digest_group<NB * NC, NA, ND, NB * NCD, 1>(
+        lane, wK, A, I, Dad, [&](int bc) { return (bc / NC) * NCD + (bc % NC) * ND; },
+        [&](int bc) { return (size_t)(fb + bc / NC) * n + fc + bc % NC; });
+    digest_group<NA * ND, NB, NC, NCD, ND>(
+        lane, wK, A, I, Dbc, [&](int ad) { return (ad / ND) * NB * NCD + ad % ND; },
+        [&](int ad) { return (size_t)(fa + ad / ND) * n + fd + ad % ND; });
+    digest_group<NB * ND, NA, NC, NB * NCD, ND>(
+        lane, wK, A, I, Dac, [&](int bd) { return (bd / ND) * NCD + bd % ND; },
+        [&](int bd) { return (size_t)(fb + bd / ND) * n + fd + bd % ND; });
     __syncwarp();
 }
 
