@@ -387,6 +387,7 @@ class GraphSCF:
         self.recaptures = 0
         self.sp2 = sp2
         self.graph = None
+        self.post_graph = None      # the post-build half alone, for the full-build cycles
 
     def _density(self, Fd, shift=None):
         torch = self.torch
@@ -471,22 +472,24 @@ class GraphSCF:
         r = self.rhf
         if guess == "sad" and D0 is None:
             D0 = r.guess("sad")
-        if guess == "core":
-            Fg = r.H
-        else:
-            dg = torch.diagonal(r.H)
-            Fg = 0.875 * r.S * (dg[:, None] + dg[None, :])
-            Fg.fill_diagonal_(0.0)
-            Fg += torch.diag(dg)
-        Fo = r.X.T @ Fg @ r.X
-        e, C = torch.linalg.eigh(Fo)
-        if self.sp2 is None:
-            self.sp2 = sp2_steps(e.cpu().numpy(), r.nocc, gershgorin_range(Fo))
-        if D0 is not None:
-            self.D.copy_(D0)
-        else:
-            Co = r.X @ C[:, : r.nocc]
-            self.D.copy_(2.0 * Co @ Co.T)
+        # the guess spectrum: the SP2 step count (set by the first solve on this
+        # molecule, raised by the defect check) and, without D0, the density
+        if self.sp2 is None or D0 is None:
+            if guess == "core":
+                Fg = r.H
+            else:
+                dg = torch.diagonal(r.H)
+                Fg = 0.875 * r.S * (dg[:, None] + dg[None, :])
+                Fg.fill_diagonal_(0.0)
+                Fg += torch.diag(dg)
+            Fo = r.X.T @ Fg @ r.X
+            e, C = torch.linalg.eigh(Fo)
+            if self.sp2 is None:
+                self.sp2 = sp2_steps(e.cpu().numpy(), r.nocc, gershgorin_range(Fo))
+            if D0 is None:
+                Co = r.X @ C[:, : r.nocc]
+                D0 = 2.0 * Co @ Co.T
+        self.D.copy_(D0)
         self.valid.zero_()
         self.cycle.zero_()
         self.errs.zero_()
@@ -513,7 +516,16 @@ class GraphSCF:
             else:
                 dD, F = st.fock_input()
                 r.eng.fock2e(dD, o=F)
-                st.step_device()
+                if graph:
+                    # the full-build cycles: the post-build half as its own graph
+                    if self.post_graph is None:
+                        torch.cuda.synchronize(r.device)
+                        self.post_graph = torch.cuda.CUDAGraph()
+                        with torch.cuda.graph(self.post_graph):
+                            self._post()
+                    self.post_graph.replay()
+                else:
+                    st.step_device()
             st.step(self.out.cpu().numpy())
         torch.cuda.synchronize(r.device)
         res = st.result()
@@ -609,6 +621,7 @@ class DeviceSCFState:
         if abs(defect) > 1e-9 * max(1, r.nocc) and g.sp2 < 200:
             g.sp2 += 16                 # the projection needs more steps for this spectrum
             g.graph = None
+            g.post_graph = None
             self.post_graph = None
             g.recaptures += 1
         if self.it >= 3 and prms < self.denserms and pchange < 100 * self.denserms:
