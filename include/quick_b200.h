@@ -230,6 +230,12 @@ int qk_fp64_peak(int device, double *gflops);
  * synchronisation, so the iteration can be captured in a CUDA graph); QUICK
  * solves the same system on the host (src/modules/quick_scf_module.f90:165-802). */
 int qk_small_solve(const double *A_dev, const double *b_dev, int n, double *x_dev, int *ok_dev, void *stream);
+/* One SP2 purification step on `stream` (no counterpart in the reference, which
+ * diagonalises): given Y and Y2 = Y Y (n x n device arrays), Yout = Y2 when
+ * |tr Y2 - nocc| < |2 tr Y - tr Y2 - nocc|, else 2Y - Y2 (Niklasson, Phys. Rev. B 66,
+ * 155115 (2002)).  Yout must not alias Y or Y2.  The traces and the update are one
+ * launch, so a captured SCF iteration holds two nodes per step (the GEMM and this). */
+int qk_sp2_step(const double *Y_dev, const double *Y2_dev, double *Yout_dev, int n, double nocc, void *stream);
 
 /* One-electron integrals on device `device` (replaces the get1e path and the
  * reference's gpu_get_oei_, src/gpu/gpu_oei.cu:194; CPU twin

@@ -8,6 +8,7 @@
 // pivot sets *ok = 0 (the caller then keeps the plain Fock matrix).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "quick_b200.h"
@@ -75,7 +76,56 @@ __global__ void __launch_bounds__(32) small_solve_kernel(const double* __restric
     }
 }
 
+// One step of SP2 purification (Niklasson, Phys. Rev. B 66, 155115 (2002)) after
+// Y2 = Y Y: Yout = Y2 when |tr Y2 - ne| < |2 tr Y - tr Y2 - ne|, else 2Y - Y2.
+// Every block sums both traces itself, in the same fixed order, so all blocks take
+// the same branch without a second launch; Yout must not alias Y or Y2.
+constexpr int kSp2Threads = 256;
+
+__global__ void __launch_bounds__(kSp2Threads) sp2_step_kernel(const double* __restrict__ Y,
+                                                               const double* __restrict__ Y2,
+                                                               double* __restrict__ Yout, int n, double ne) {
+    __shared__ double part[2][kSp2Threads / 32];
+    __shared__ int square;
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < n; i += kSp2Threads) {
+        t0 += Y[(size_t)i * (n + 1)];
+        t1 += Y2[(size_t)i * (n + 1)];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        t0 += __shfl_xor_sync(0xffffffffu, t0, o);
+        t1 += __shfl_xor_sync(0xffffffffu, t1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        part[0][threadIdx.x >> 5] = t0;
+        part[1][threadIdx.x >> 5] = t1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int w = 0; w < kSp2Threads / 32; ++w) {
+            s0 += part[0][w];
+            s1 += part[1][w];
+        }
+        square = fabs(s1 - ne) < fabs(2.0 * s0 - s1 - ne);
+    }
+    __syncthreads();
+    const bool sq = square != 0;
+    const size_t nn = (size_t)n * n;
+    for (size_t k = (size_t)blockIdx.x * kSp2Threads + threadIdx.x; k < nn; k += (size_t)gridDim.x * kSp2Threads)
+        Yout[k] = sq ? Y2[k] : 2.0 * Y[k] - Y2[k];
+}
+
 }  // namespace qk
+
+extern "C" int qk_sp2_step(const double* Y, const double* Y2, double* Yout, int n, double nocc, void* stream) {
+    if (!Y || !Y2 || !Yout || n < 1 || Yout == Y || Yout == Y2) return QK_ERR_INVALID_ARG;
+    const size_t nn = (size_t)n * n;
+    const int grid = (int)std::min<size_t>(4 * 148, (nn + qk::kSp2Threads - 1) / qk::kSp2Threads);
+    qk::sp2_step_kernel<<<grid, qk::kSp2Threads, 0, (cudaStream_t)stream>>>(Y, Y2, Yout, n, nocc);
+    return cudaGetLastError() == cudaSuccess ? QK_OK : QK_ERR_CUDA;
+}
 
 extern "C" int qk_small_solve(const double* A, const double* b, int n, double* x, int* ok, void* stream) {
     if (!A || !b || !x || !ok || n < 1 || n > qk::kSmallSolveMax) return QK_ERR_INVALID_ARG;

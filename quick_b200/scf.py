@@ -378,6 +378,7 @@ class GraphSCF:
         self.ok = torch.zeros(1, dtype=torch.int32, device=dev)
         self.eye_k = torch.eye(k, dtype=dt, device=dev)
         self.eye_m = torch.eye(m, dtype=dt, device=dev)
+        self.Ya, self.Yb, self.Y2 = z(m, m), z(m, m), z(m, m)   # SP2 iterates (ping-pong) and Y Y
         self.out = z(4)
         self.cycle = torch.zeros((), dtype=torch.int64, device=dev)
         self.XtS = rhf.X.T @ rhf.S          # orthogonal-basis projector of D: (XtS) D (XtS)^T / 2
@@ -401,12 +402,18 @@ class GraphSCF:
         d = torch.diagonal(Fo)
         rad = torch.abs(Fo).sum(dim=1) - torch.abs(d)
         emin, emax = torch.min(d - rad), torch.max(d + rad)
-        Y = (emax * self.eye_m - Fo) / (emax - emin)
         ne = float(self.rhf.nocc)
+        cur, nxt = self.Ya, self.Yb
+        torch.div(emax * self.eye_m - Fo, emax - emin, out=cur)
+        # each step: one GEMM and one fused trace-test-and-update launch
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.rhf.device).cuda_stream)
+        m = cur.shape[0]
         for _ in range(self.sp2):
-            Y2 = Y @ Y
-            t0, t1 = torch.trace(Y), torch.trace(Y2)
-            Y = torch.where(torch.abs(t1 - ne) < torch.abs(2.0 * t0 - t1 - ne), Y2, 2.0 * Y - Y2)
+            torch.mm(cur, cur, out=self.Y2)
+            check(lib().qk_sp2_step(ctypes.c_void_p(cur.data_ptr()), ctypes.c_void_p(self.Y2.data_ptr()),
+                                    ctypes.c_void_p(nxt.data_ptr()), m, ne, stream), "qk_sp2_step")
+            cur, nxt = nxt, cur
+        Y = cur
         # idempotency defect tr(Y - Y^2): zero once the projection has converged
         self.out[3].copy_(torch.trace(Y) - torch.sum(Y * Y))
         return 2.0 * (X @ Y @ X.T)

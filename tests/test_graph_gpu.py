@@ -59,6 +59,25 @@ def test_small_solve_diis_shape_and_singular():
     assert ok == 0 and not x.any()
 
 
+@pytest.mark.parametrize("n,nocc", [(1, 0.0), (37, 5.0), (37, 30.0), (300, 41.0)])
+def test_sp2_step_matches_formula(n, nocc):
+    """qk_sp2_step against the step written out in torch, both branches."""
+    _cuda()
+    from quick_b200._native import check, lib
+    g = torch.Generator().manual_seed(n)
+    A = torch.randn(n, n, generator=g, dtype=torch.float64)
+    Y = ((A + A.T) / (4.0 * n ** 0.5) + 0.5 * torch.eye(n, dtype=torch.float64)).cuda()
+    Y2 = Y @ Y
+    out = torch.full_like(Y, float("nan"))
+    s = torch.cuda.current_stream()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    check(lib().qk_sp2_step(vp(Y), vp(Y2), vp(out), n, nocc, ctypes.c_void_p(s.cuda_stream)), "qk_sp2_step")
+    t0, t1 = float(torch.trace(Y)), float(torch.trace(Y2))
+    want = Y2 if abs(t1 - nocc) < abs(2.0 * t0 - t1 - nocc) else 2.0 * Y - Y2
+    assert torch.equal(out, want)
+    assert lib().qk_sp2_step(vp(Y), vp(Y2), vp(Y), n, nocc, ctypes.c_void_p(s.cuda_stream)) != 0   # aliasing refused
+
+
 def test_sp2_projector_equals_diagonalisation():
     _cuda()
     from quick_b200.scf import RHF, GraphSCF, gershgorin_range, sp2_steps
