@@ -433,7 +433,7 @@ def run_ours(args):
                          "timing": "dominant class kernel timed alone with CUDA events, mean of "
                                    f"{nprof} builds; all_classes_tflops uses the concurrent build time"},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": 8 * n * n,
+            "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": 16 * n * n,
                     "d2h_bytes_per_step": 8 * n * n},
             "gpu_launches": int(launches) * args.steps,
             "clocks": clk,

@@ -141,7 +141,8 @@ int qk_last_work_mixed(qk_ctx *ctx, long long *quartets_fp32);
  * host and waits for their upload. */
 int qk_fock2e_device(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
                      double *o_dev, void *stream);
-/* Same with host buffers (copies D in, adds G into o, synchronises). */
+/* Same with host buffers: D and o are copied to the device, G is added into o there
+ * and o is copied back; synchronises.  Pinned host buffers make the copies fastest. */
 int qk_fock2e_host(qk_ctx *ctx, const double *D, const double *cutmat, double *o);
 /* Density screen on the device: cutmat_dev(nshell,nshell) = max |D| per shell pair
  * (stream: a cudaStream_t, NULL = the CUDA default stream). */

@@ -1937,8 +1937,10 @@ int qk_fock2e_host(qk_ctx* c, const double* D, const double* cutmat, double* o) 
     cudaStream_t s = c->stream;
     QK_CUDA_TRY(c->d_D.reserve((size_t)n * n));
     QK_CUDA_TRY(c->d_o.reserve((size_t)n * n));
+    // o goes up with D and comes back with G added on the device: no host-side
+    // staging buffer and no host loop
     QK_CUDA_TRY(cudaMemcpyAsync(c->d_D.p, D, sizeof(double) * n * n, cudaMemcpyHostToDevice, s));
-    QK_CUDA_TRY(cudaMemsetAsync(c->d_o.p, 0, sizeof(double) * n * n, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(c->d_o.p, o, sizeof(double) * n * n, cudaMemcpyHostToDevice, s));
     const double* cm = nullptr;
     if (cutmat) {
         QK_CUDA_TRY(c->d_cutmat.reserve((size_t)ns * ns));
@@ -1947,10 +1949,8 @@ int qk_fock2e_host(qk_ctx* c, const double* D, const double* cutmat, double* o) 
     }
     int st = fock2e_device(c, c->d_D.p, cm, c->d_o.p, s);
     if (st) return st;
-    std::vector<double> G((size_t)n * n);
-    QK_CUDA_TRY(cudaMemcpyAsync(G.data(), c->d_o.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(o, c->d_o.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, s));
     QK_CUDA_TRY(cudaStreamSynchronize(s));
-    for (size_t i = 0; i < G.size(); ++i) o[i] += G[i];
     return QK_OK;
 }
 
