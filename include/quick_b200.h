@@ -164,6 +164,22 @@ int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_de
 int qk_fock2e_device_noalloc(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev,
                              double *o_dev, void *stream);
 
+/* Sharded builds (the GPU form of the reference's MPI split of the work by cost,
+ * MPI_setup_hfoperator, src/mpi_setup.f90:295-354, which deals bra shells to ranks greedily).
+ * qk_set_shard: this context keeps every count-th work item (rank, rank + count, ...)
+ * of each class's cost-ordered list; (0, 1) = all of them (the default).  The work
+ * lists are rebuilt at the next build.
+ * qk_fock2e_device_accumulate: the context's share of the build of G(D_dev) added
+ * into A_dev, the caller's int64 fixed-point accumulator (nbasis^2 on the device,
+ * 2^-44 units, cleared by the caller); nothing is finalised.  Summing the ranks'
+ * accumulators (an integer all-reduce, exact and order-free) and calling
+ * qk_finalize_fixed once gives, bit for bit, the unsharded build.
+ * qk_finalize_fixed: o_dev(n,n) += (A + A^T) * 2^-44 on `stream`. */
+int qk_set_shard(qk_ctx *ctx, int rank, int count);
+int qk_fock2e_device_accumulate(qk_ctx *ctx, const double *D_dev, const double *cutmat_dev, long long *A_dev,
+                                void *stream);
+int qk_finalize_fixed(const long long *A_dev, int n, double *o_dev, void *stream);
+
 /* Build the shell-pair tables and work lists for the current basis, Schwarz bounds,
  * cutoffs and precision now (the first Fock build does it otherwise), e.g. while
  * other work keeps the GPU busy.  Uses only the context's own stream. */

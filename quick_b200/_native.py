@@ -23,7 +23,7 @@ EXPORTED = [
     "qk_last_work", "qk_launches_per_build", "qk_oei_host", "qk_set_profiling",
     "qk_class_profile", "qk_fp64_peak", "qk_fock2e_device_noalloc", "qk_set_precision",
     "qk_last_work_mixed", "qk_batch_create", "qk_batch_destroy", "qk_batch_fock2e",
-    "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_sp2_step", "qk_set_streams",
+    "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_sp2_step", "qk_set_shard", "qk_fock2e_device_accumulate", "qk_finalize_fixed", "qk_set_streams",
     "qk_set_class_launch", "qk_class_launch", "qk_batch_reserve_sms",
 ]
 
@@ -86,6 +86,9 @@ def lib():
     L.qk_class_launch.argtypes = [P, I, PI, PI, PI, PI]
     L.qk_small_solve.argtypes = [P, P, I, P, P, P]
     L.qk_sp2_step.argtypes = [P, P, P, I, ctypes.c_double, P]
+    L.qk_set_shard.argtypes = [P, I, I]
+    L.qk_fock2e_device_accumulate.argtypes = [P, P, P, P, P]
+    L.qk_finalize_fixed.argtypes = [P, I, P, P]
     L.qk_device_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
     for name in EXPORTED:
         if name.startswith("gpu_"):

@@ -1051,6 +1051,7 @@ struct qk_ctx {
     double integralCutoff = 1e-7, primLimit = 1e-8;
     double fp32_bound = 0.0;          // mixed form: FP32 below this Schwarz bound product
     int nstreams = 4;                 // class kernels run over this many streams (0: one after another)
+    int shard_rank = 0, shard_count = 1;   // this context's share of the work items (qk_set_shard)
     int cls_wpb[qk::kNumClasses] = {};    // warps per block of each class launch (0: default)
     int cls_bpsm[qk::kNumClasses] = {};   // cap on resident blocks per SM (0: as many as fit)
     double built_fp32 = -1.0;
@@ -1368,6 +1369,20 @@ static int build_work(qk_ctx* c) {
             if (x.it.w != y.it.w) return x.it.w < y.it.w;
             return x.cost > y.cost;
         });
+        // a shard keeps every shard_count-th item of the cost-ordered list (each
+        // precision part stays cost-ordered), so the shards' work is balanced
+        if (c->shard_count > 1) {
+            size_t k = 0;
+            for (size_t i = 0; i < tmp.size(); ++i)
+                if ((int)(i % (size_t)c->shard_count) == c->shard_rank) tmp[k++] = tmp[i];
+            tmp.resize(k);
+            W.nquart = W.nprimq = W.nquart32 = 0;
+            for (const Tmp& t : tmp) {
+                W.nquart += t.it.z;
+                W.nprimq += t.cost * t.it.z;
+                if (t.it.w == 1) W.nquart32 += t.it.z;
+            }
+        }
         W.n64 = 0;
         for (const Tmp& t : tmp) W.n64 += t.it.w == 0;
         W.items.resize(tmp.size());
@@ -1432,7 +1447,11 @@ static void launch_class(const ClassEntry& ce, const ClassWork& W, cudaStream_t 
               counters + kNumClasses + ci);
 }
 
-static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s) {
+// A_ext: the caller's int64 accumulator (nbasis^2, not cleared, not finalised)
+// instead of the context's, for sharded builds whose accumulators are summed
+// across GPUs before the one finalisation; o is then unused.
+static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s,
+                         unsigned long long* A_ext = nullptr) {
     int st = ensure_pairs(c);
     if (st) return st;
     const int n = c->nbasis, ns = c->nshell;
@@ -1443,14 +1462,16 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         QK_CUDA_TRY(cudaGetLastError());
         cutmat = c->d_cutmat.p;
     }
-    QK_CUDA_TRY(c->d_A.reserve((size_t)n * n));
     QK_CUDA_TRY(c->d_counters.reserve(2 * kNumClasses));
-    QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * n * n, s));
+    if (!A_ext) {
+        QK_CUDA_TRY(c->d_A.reserve((size_t)n * n));
+        QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * n * n, s));
+    }
     QK_CUDA_TRY(cudaMemsetAsync(c->d_counters.p, 0, sizeof(int) * 2 * kNumClasses, s));
     DevData d = make_devdata(c);
     d.D = D;
     d.cutmat = cutmat;
-    d.A = c->d_A.p;
+    d.A = A_ext ? A_ext : c->d_A.p;
     d.stats = nullptr;
     if (c->profile_stats) {
         QK_CUDA_TRY(c->d_stats.reserve(2 * kNumClasses));
@@ -1495,8 +1516,10 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
                 QK_CUDA_TRY(cudaEventRecord(c->join_ev[k], c->aux[k]));
                 QK_CUDA_TRY(cudaStreamWaitEvent(s, c->join_ev[k], 0));
             }
-    finalize_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(c->d_A.p, n, o);
-    QK_CUDA_TRY(cudaGetLastError());
+    if (!A_ext) {
+        finalize_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(c->d_A.p, n, o);
+        QK_CUDA_TRY(cudaGetLastError());
+    }
     c->last_quart = nq;
     c->last_primq = npq;
     return QK_OK;
@@ -1965,6 +1988,34 @@ int qk_fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutmat, d
     std::lock_guard<std::mutex> g(c->mu);
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
     return fock2e_device_noalloc(c, D, cutmat, o, (cudaStream_t)stream);
+}
+
+
+// ------------------------------------------------------------- sharded builds (C ABI)
+int qk_set_shard(qk_ctx* c, int rank, int count) {
+    if (!c || count < 1 || rank < 0 || rank >= count) return fail(QK_ERR_INVALID_ARG, "qk_set_shard: bad rank/count");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (c->shard_rank != rank || c->shard_count != count) {
+        c->shard_rank = rank;
+        c->shard_count = count;
+        c->pairs_dirty = true;
+    }
+    return QK_OK;
+}
+
+int qk_fock2e_device_accumulate(qk_ctx* c, const double* D, const double* cutmat, long long* A, void* stream) {
+    if (!c || !D || !A) return fail(QK_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    return fock2e_device(c, D, cutmat, nullptr, (cudaStream_t)stream, reinterpret_cast<unsigned long long*>(A));
+}
+
+int qk_finalize_fixed(const long long* A, int n, double* o, void* stream) {
+    if (!A || !o || n < 1) return fail(QK_ERR_INVALID_ARG, "qk_finalize_fixed: bad argument");
+    finalize_kernel<<<(n * n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const unsigned long long*>(A), n, o);
+    QK_CUDA_TRY(cudaGetLastError());
+    return QK_OK;
 }
 
 

@@ -152,6 +152,50 @@ class Get2e:
         check(lib().qk_fock2e_host(self.h, _p(D), cm, _p(out)), "qk_fock2e_host")
         return out
 
+    # -- sharded builds (one molecule over several GPUs)
+    def set_shard(self, rank: int, count: int):
+        """Keep every ``count``-th work item of each class, starting at ``rank``
+        ((0, 1) = all); the work lists are rebuilt at the next build."""
+        check(lib().qk_set_shard(self.h, int(rank), int(count)), "qk_set_shard")
+
+    def accumulate(self, D, A, cutmat=None, stream=None):
+        """This context's share of G(D) added into ``A``: an int64 (nbasis, nbasis)
+        CUDA tensor of fixed-point sums (2^-44 units) that the caller clears."""
+        import torch
+        n = self.basis.nbasis
+        if D.shape != (n, n) or A.shape != (n, n) or A.dtype != torch.int64 or not A.is_contiguous():
+            raise ValueError("accumulate: D must be (n, n) float64 and A a contiguous (n, n) int64 tensor")
+        D = D.contiguous()
+        s = stream if stream is not None else torch.cuda.current_stream(D.device)
+        cm = ctypes.c_void_p(cutmat.data_ptr()) if cutmat is not None else None
+        check(lib().qk_fock2e_device_accumulate(self.h, ctypes.c_void_p(D.data_ptr()), cm,
+                                                ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(s.cuda_stream)),
+              "qk_fock2e_device_accumulate")
+        return A
+
+    def fock2e_sharded(self, D, o=None, group=None):
+        """o += G(D) with the work split over the ranks of ``group`` (torch.distributed,
+        one rank per GPU): each rank builds its share into an int64 accumulator, one
+        integer all-reduce sums them (exact, so the result equals the one-GPU build bit
+        for bit), and every rank finalises the same o.  Call ``set_shard(rank, size)``
+        first (``shard_for``)."""
+        import torch
+        n = self.basis.nbasis
+        if o is None:
+            o = torch.zeros((n, n), dtype=torch.float64, device=D.device)
+        A = torch.zeros((n, n), dtype=torch.int64, device=D.device)
+        self.accumulate(D, A)
+        allreduce_fixed(A, group)
+        s = torch.cuda.current_stream(D.device)
+        check(lib().qk_finalize_fixed(ctypes.c_void_p(A.data_ptr()), n, ctypes.c_void_p(o.data_ptr()),
+                                      ctypes.c_void_p(s.cuda_stream)), "qk_finalize_fixed")
+        return o
+
+    def shard_for(self, group=None):
+        """set_shard(rank, world size) of ``group``."""
+        import torch.distributed as dist
+        self.set_shard(dist.get_rank(group), dist.get_world_size(group))
+
     def set_streams(self, nstreams: int):
         """Class kernels over ``nstreams`` concurrent streams (0: one after another)."""
         check(lib().qk_set_streams(self.h, int(nstreams)), "qk_set_streams")
@@ -243,6 +287,17 @@ class Get2eBatch:
 # ---------------------------------------------------------------------------
 # The reference's Fortran -> C call sequence (all arguments by reference).
 # ---------------------------------------------------------------------------
+def allreduce_fixed(A, group=None):
+    """Sum int64 fixed-point accumulators over the ranks of ``group`` in place (a
+    no-op without an initialised process group).  Integer addition is exact and
+    order-free, so every rank ends with the same bits whatever the reduction order
+    (NCCL on GPUs, gloo on CPUs)."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(A, op=dist.ReduceOp.SUM, group=group)
+    return A
+
+
 def _ref(x, ctype):
     return ctypes.byref(ctype(x))
 

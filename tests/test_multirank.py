@@ -1,7 +1,8 @@
 """World-size-2 tests of the multi-process logic on CPU (gloo): the job time is
 the maximum over ranks, and a Fock build split over ranks by strided bra shells
 (the reference's MPI split, src/mpi_setup.f90:295-354) sums back to the full
-build after one all-reduce -- the plan for splitting one build over GPUs."""
+build after one all-reduce, and the int64 all-reduce that joins the shards of
+a GPU build (Get2e.fock2e_sharded) is exact."""
 import os
 import socket
 
@@ -46,7 +47,14 @@ def _worker(rank, world, port, q):
         G = torch.tensor(G_part)
         dist.all_reduce(G)
         G_full, _ = orc.get2e(D, cm, Y, cp, 1e-10, 1e-11)
-        q.put((rank, t, float(np.abs(G.numpy() - G_full).max())))
+        # 3. the sharded GPU build's collective: int64 fixed-point accumulators summed
+        #    exactly (quick_b200.get2e.allreduce_fixed, as Get2e.fock2e_sharded calls it)
+        from quick_b200.get2e import allreduce_fixed
+        parts = [np.random.default_rng(r).integers(-2 ** 52, 2 ** 52, size=(7, 7)) for r in range(world)]
+        A = torch.tensor(parts[rank], dtype=torch.int64)
+        allreduce_fixed(A)
+        exact = bool((A.numpy() == parts[0] + parts[1]).all())
+        q.put((rank, t, float(np.abs(G.numpy() - G_full).max()), exact))
     finally:
         dist.destroy_process_group()
 
@@ -62,6 +70,7 @@ def test_two_ranks_gloo():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, t, err in out:
+    for rank, t, err, exact in out:
         assert t == 15.0
         assert err <= 1e-13
+        assert exact
