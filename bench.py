@@ -9,7 +9,7 @@ core-Hamiltonian guess density (idempotent, 320 electrons), synthetic data.
 Prints ONE JSON line (rank 0).  ``value`` is Fock builds/s with inputs resident
 on the device (CUDA events on the launching stream, L2 flushed between steps);
 ``e2e`` is the same metric through the host-buffer C ABI (qk_fock2e_host) with
-the density copied in and G copied out every step.  ``roofline`` is the
+pinned host buffers: the density and o copied in, o + G copied out every step.  ``roofline`` is the
 dominant class kernel against the in-run FP64 FMA peak.  ``cpu_baseline`` is the
 C++ oracle (a restatement of the reference's CPU get2e) on a bounded sample.
 
