@@ -157,7 +157,9 @@ int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_de
  * every GPU loading it holds until exit: limits nbasis <= 1024 and, with
  * cutmat_dev == NULL, nshell <= 512; larger sizes return QK_ERR_INVALID_ARG.
  * The pair tables must already exist: run qk_fock2e_device (or qk_prepare) once after
- * any basis or Schwarz change or a tightening of the cutoff, else QK_ERR_NOT_READY.  The first call on a device looks
+ * any basis or Schwarz change, a tightening of the cutoff or a change of the FP32 bound
+ * (qk_set_precision), else QK_ERR_NOT_READY.  The launch shape follows qk_set_streams,
+ * and qk_last_work reports this build's counts.  The first call on a device looks
  * up the array's device address; make it before any stream capture.  All calls share
  * the array, so calls that overlap on the GPU race: keep them on one stream (or order
  * them with events). */
@@ -168,7 +170,9 @@ int qk_fock2e_device_noalloc(qk_ctx *ctx, const double *D_dev, const double *cut
  * MPI_setup_hfoperator, src/mpi_setup.f90:295-354, which deals bra shells to ranks greedily).
  * qk_set_shard: this context keeps every count-th work item (rank, rank + count, ...)
  * of each class's cost-ordered list; (0, 1) = all of them (the default).  The work
- * lists are rebuilt at the next build.
+ * lists are rebuilt at the next build.  While count > 1 the finalising builds
+ * (qk_fock2e_device, qk_fock2e_host, qk_fock2e_device_noalloc, qk_batch_fock2e) refuse
+ * the context with QK_ERR_INVALID_ARG: they would return only this shard's part of G.
  * qk_fock2e_device_accumulate: the context's share of the build of G(D_dev) added
  * into A_dev, the caller's int64 fixed-point accumulator (nbasis^2 on the device,
  * 2^-44 units, cleared by the caller); nothing is finalised.  Summing the ranks'
@@ -240,6 +244,12 @@ int qk_class_profile(qk_ctx *ctx, int max_classes, int *cls, float *ms, long lon
                      double *prim_flops, double *quartet_flops);
 /* FP64 FMA throughput of device `device` measured by a short probe kernel (GFLOP/s). */
 int qk_fp64_peak(int device, double *gflops);
+/* Diagnostic: the Boys function F_0..F_M (M <= 4 * qk_max_l()) at n points T[i] >= 0
+ * (host arrays), evaluated on the device by the two forms the Fock kernels use: the
+ * per-lane kernels' row-table Taylor/downward-recursion evaluation (F_rows) and the
+ * cooperative kernels' one-m evaluation (F_one); out[i*(M+1) + m].  No counterpart in
+ * the reference, whose device Boys is src/gpu/gpu_fmt.h:5-72.  Synchronises. */
+int qk_boys(qk_ctx *ctx, int M, const double *T, int n, double *F_rows, double *F_one);
 
 /* Solve the n x n system A x = b (row-major device arrays, n <= 64) on `stream`
  * with partial pivoting, in one warp; *ok_dev = 1, or 0 (and x = 0) when a pivot

@@ -23,7 +23,8 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_LIB_V3 = os.path.join(_HERE, "_build", "liboracle.so")       # AVX2/FMA (x86-64-v3)
+_LIB_V4 = os.path.join(_HERE, "_build", "liboracle_v4.so")    # AVX-512 (x86-64-v4)
 _lib = None
 
 
@@ -31,12 +32,31 @@ def build():
     subprocess.run(["make", "-C", _HERE, "-s"], check=True)
 
 
+def host_isa() -> str:
+    """'v4' when the host CPU has the AVX-512 subsets of x86-64-v4, else 'v3'."""
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("flags"):
+                    flags = set(ln.split(":", 1)[1].split())
+                    break
+        return "v4" if {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags else "v3"
+    except OSError:
+        return "v3"
+
+
+def lib_path() -> str:
+    return _LIB_V4 if host_isa() == "v4" else _LIB_V3
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+        path = lib_path()
+        if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
+        L = ctypes.CDLL(path)
         P = ctypes.c_void_p
         I = ctypes.c_int
         D = ctypes.c_double

@@ -880,6 +880,32 @@ __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
     if (r == 12345.678) out[0] = r;   // keeps the chains live
 }
 
+// Boys function probe: F_0..F_M at each T by the two device forms the Fock
+// kernels use -- the per-lane row-table evaluation (boys_scaled_rows<M>, scale 1)
+// and the cooperative kernels' one-m evaluation (boys_one) -- for testing them
+// directly against high-precision values.
+template <int M>
+__global__ void boys_probe_kernel(const double* __restrict__ T, int n, const double2* __restrict__ rows8,
+                                  const double* __restrict__ tab, double* __restrict__ f_rows,
+                                  double* __restrict__ f_one) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double F[M + 1];
+    boys_scaled_rows<M>(T[i], 1.0, rows8 + (size_t)M * kBoysNT * (kBoysRow / 2), F);
+#pragma unroll
+    for (int m = 0; m <= M; ++m) {
+        f_rows[(size_t)i * (M + 1) + m] = F[m];
+        f_one[(size_t)i * (M + 1) + m] = boys_one(m, T[i], tab);
+    }
+}
+
+template <int M>
+static cudaError_t launch_boys_probe(const double* T, int n, const double2* rows8, const double* tab, double* fr,
+                                     double* fo, cudaStream_t s) {
+    boys_probe_kernel<M><<<(n + 127) / 128, 128, 0, s>>>(T, n, rows8, tab, fr, fo);
+    return cudaGetLastError();
+}
+
 __global__ void finalize_kernel(const unsigned long long* __restrict__ A, int n, double* __restrict__ o) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n * n) return;
@@ -1452,6 +1478,10 @@ static void launch_class(const ClassEntry& ce, const ClassWork& W, cudaStream_t 
 // across GPUs before the one finalisation; o is then unused.
 static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s,
                          unsigned long long* A_ext = nullptr) {
+    // a sharded context holds only its share of the work: finalising that share
+    // into o would be a silently partial Fock matrix
+    if (!A_ext && c->shard_count > 1)
+        return fail(QK_ERR_INVALID_ARG, "context is sharded (qk_set_shard): use qk_fock2e_device_accumulate");
     int st = ensure_pairs(c);
     if (st) return st;
     const int n = c->nbasis, ns = c->nshell;
@@ -1571,16 +1601,22 @@ static int noalloc_scratch(int device, unsigned long long** out) {
 // The same build as fock2e_device with its scratch taken from g_noalloc_scratch;
 // it calls no allocator.  The pair tables and work lists must already exist.
 static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s) {
+    if (c->shard_count > 1)
+        return fail(QK_ERR_INVALID_ARG, "context is sharded (qk_set_shard): use qk_fock2e_device_accumulate");
     if (c->nbasis > kNoAllocMaxNbasis)
         return fail(QK_ERR_INVALID_ARG, "qk_fock2e_device_noalloc: nbasis exceeds the fixed scratch (max 1024)");
     if (!cutmat && c->nshell > kNoAllocMaxNshell)
         return fail(QK_ERR_INVALID_ARG,
                     "qk_fock2e_device_noalloc: nshell exceeds the fixed density-screen scratch (max 512); "
                     "pass cutmat_dev");
-    if (!c->have_basis || !c->have_schwarz || c->pairs_dirty || c->built_cut > c->integralCutoff)
+    // the same test as ensure_pairs: anything that would make qk_fock2e_device rebuild
+    // its lists (basis, Schwarz bounds, shard, a tighter cutoff, another FP32 bound)
+    // is a refusal here, since building them allocates
+    if (!c->have_basis || !c->have_schwarz || c->pairs_dirty || c->built_cut > c->integralCutoff ||
+        c->built_fp32 != c->fp32_bound)
         return fail(QK_ERR_NOT_READY,
-                    "qk_fock2e_device_noalloc: pair tables not built for the current basis/Schwarz/cutoffs; "
-                    "run qk_fock2e_device once first");
+                    "qk_fock2e_device_noalloc: pair tables not built for the current basis/Schwarz/cutoffs/"
+                    "precision; run qk_fock2e_device (or qk_prepare) once first");
     unsigned long long* base = nullptr;
     int st = noalloc_scratch(c->device, &base);
     if (st) return st;
@@ -1602,28 +1638,40 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
     d.cutmat = cutmat;
     d.A = A;
     d.stats = nullptr;
-    QK_CUDA_TRY(cudaEventRecord(c->fork_ev, s));
+    // the launch shape of fock2e_device: concurrent over the context's nstreams
+    // auxiliary streams, or one class after another on `s` (nstreams 0)
+    const bool concurrent = c->nstreams > 0;
+    if (concurrent) QK_CUDA_TRY(cudaEventRecord(c->fork_ev, s));
     bool used[qk_ctx::kAux] = {};
     int slot = 0;
+    long long nq = 0, npq = 0;
     for (int ci : c->launch_order) {
         const ClassWork& W = c->work[ci];
-        const int k = slot++ % qk_ctx::kAux;
-        cudaStream_t ls = c->aux[k];
-        if (!used[k]) {
-            QK_CUDA_TRY(cudaStreamWaitEvent(ls, c->fork_ev, 0));
-            used[k] = true;
+        cudaStream_t ls = s;
+        if (concurrent) {
+            const int k = slot++ % c->nstreams;
+            ls = c->aux[k];
+            if (!used[k]) {
+                QK_CUDA_TRY(cudaStreamWaitEvent(ls, c->fork_ev, 0));
+                used[k] = true;
+            }
         }
         const ClassEntry& ce = g_classes[ci];
         launch_class(ce, W, ls, d, counters, ci);
         QK_CUDA_TRY(cudaGetLastError());
+        nq += W.nquart;
+        npq += W.nprimq;
     }
-    for (int k = 0; k < qk_ctx::kAux; ++k)
-        if (used[k]) {
-            QK_CUDA_TRY(cudaEventRecord(c->join_ev[k], c->aux[k]));
-            QK_CUDA_TRY(cudaStreamWaitEvent(s, c->join_ev[k], 0));
-        }
+    if (concurrent)
+        for (int k = 0; k < qk_ctx::kAux; ++k)
+            if (used[k]) {
+                QK_CUDA_TRY(cudaEventRecord(c->join_ev[k], c->aux[k]));
+                QK_CUDA_TRY(cudaStreamWaitEvent(s, c->join_ev[k], 0));
+            }
     finalize_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(A, n, o);
     QK_CUDA_TRY(cudaGetLastError());
+    c->last_quart = nq;
+    c->last_primq = npq;
     return QK_OK;
 }
 
@@ -2087,6 +2135,7 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
         qk_ctx* c = ctxs[m];
         if (!c || !D[m] || !o[m]) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: null molecule entry");
         if (c->device != b->device) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: context on another device");
+        if (c->shard_count > 1) return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: context is sharded (qk_set_shard)");
         for (int j = 0; j < m; ++j)
             if (ctxs[j] == c)
                 return fail(QK_ERR_INVALID_ARG, "qk_batch_fock2e: a context appears twice (its accumulator is shared)");
@@ -2351,6 +2400,43 @@ int qk_fp64_peak(int device, double* gflops) {
     cudaEventDestroy(e1);
     const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
     *gflops = flops / (best * 1e-3) * 1e-9;
+    return QK_OK;
+}
+
+
+int qk_boys(qk_ctx* c, int M, const double* T, int n, double* F_rows, double* F_one) {
+    if (!c || !T || !F_rows || !F_one || n < 1 || M < 0 || M > 4 * kMaxL)
+        return fail(QK_ERR_INVALID_ARG, "qk_boys: bad argument");
+    for (int i = 0; i < n; ++i)
+        if (!(T[i] >= 0.0)) return fail(QK_ERR_INVALID_ARG, "qk_boys: T must be >= 0");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    cudaStream_t s = c->stream;
+    const size_t nout = (size_t)n * (M + 1);
+    DevBuf<double> dT, dr, d1;
+    QK_CUDA_TRY(dT.reserve(n));
+    QK_CUDA_TRY(dr.reserve(nout));
+    QK_CUDA_TRY(d1.reserve(nout));
+    QK_CUDA_TRY(cudaMemcpyAsync(dT.p, T, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    const double2* rows8 = (const double2*)c->d_boys8.p;
+    const double* tab = c->d_boys.p;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (M) {
+#define QK_BOYS_CASE(m) case m: e = launch_boys_probe<m>(dT.p, n, rows8, tab, dr.p, d1.p, s); break;
+        QK_BOYS_CASE(0) QK_BOYS_CASE(1) QK_BOYS_CASE(2) QK_BOYS_CASE(3) QK_BOYS_CASE(4)
+#if QK_MAX_L >= 2
+        QK_BOYS_CASE(5) QK_BOYS_CASE(6) QK_BOYS_CASE(7) QK_BOYS_CASE(8)
+#endif
+#if QK_MAX_L >= 3
+        QK_BOYS_CASE(9) QK_BOYS_CASE(10) QK_BOYS_CASE(11) QK_BOYS_CASE(12)
+#endif
+#undef QK_BOYS_CASE
+        default: break;
+    }
+    QK_CUDA_TRY(e);
+    QK_CUDA_TRY(cudaMemcpyAsync(F_rows, dr.p, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(F_one, d1.p, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaStreamSynchronize(s));
     return QK_OK;
 }
 

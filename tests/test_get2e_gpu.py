@@ -167,7 +167,7 @@ def test_golden_energy_gpu():
         return eng.fock2e(torch.tensor(D, device="cuda"), cutmat=torch.tensor(cm, device="cuda")).cpu().numpy()
 
     got = O.rhf(b, guess="gwh", fock_builder=fb)
-    assert abs(got["E"] - (-75.983996360)) <= 1e-6
+    assert abs(got["E"] - (-75.983996360)) <= 2e-7      # the oracle measures 1.6e-8
     eng.close()
 
 

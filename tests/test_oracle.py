@@ -64,6 +64,12 @@ def test_alkane_geometry():
     assert abs(cc.mean() - 1.54) < 0.02
 
 
+# measured |E_oracle - E_golden| above 2.5e-7 Eh: CaCl2/3-21G 1.6e-5, CaCl2/STO-3G
+# 9.3e-7, HI/STO-3G 6.3e-7, HI/3-21G 3.3e-7 (heavy atoms; the saved outputs come
+# from the reference's GPU build)
+GOLDEN_EXCEPTIONS = {"ene_CaCl2_rhf_321g": 2e-5, "ene_CaCl2_rhf_sto3g": 1e-6, "ene_HI_rhf_sto3g": 7e-7,
+                     "ene_HI_rhf_321g": 4e-7}
+
 FAST = [c for c in GOLDEN if c["name"].startswith("ene_") and "psb5" not in c["name"]
         and "PO4" not in c["name"] and "acetone" not in c["name"]]
 
@@ -75,9 +81,11 @@ def test_oracle_scf_golden(case):
     # QUICK starts from the SAD guess; here the lower of the two simple guesses picks
     # the ground state (a single guess can land in an excited SCF solution)
     r = min((O.rhf(b, guess=g, nthreads=2) for g in ("core", "gwh")), key=lambda x: x["E"])
-    # the reference's harness compares at 4e-5 (tools/runtest:867); the goldens were
-    # mostly produced by the reference's GPU build, whose screening differs slightly
-    tol = 4e-5 if case["name"] == "ene_CaCl2_rhf_321g" else 2e-6
+    # 71 of the 77 agree within 2e-7 Eh; the bound is 2.5e-7 (SiH4 measures 2.3e-7)
+    # except for the named cases below, whose measured differences are kept as their
+    # bounds.  The reference's own harness compares at 4e-5 (tools/runtest:867); the
+    # goldens were mostly written by its GPU build, whose screening differs slightly.
+    tol = GOLDEN_EXCEPTIONS.get(case["name"], 2.5e-7)
     assert abs(r["E"] - case["total_energy"]) <= tol, (r["E"], case["total_energy"])
 
 
@@ -87,7 +95,7 @@ def test_oracle_scf_golden_larger(name):
     case = [c for c in GOLDEN if c["name"] == name][0]
     m = Molecule.from_angstrom([a[0] for a in case["atoms"]], [a[1:] for a in case["atoms"]], case["charge"])
     r = O.rhf(build_basis(m, case["basis"]), guess="gwh")
-    assert abs(r["E"] - case["total_energy"]) <= 1e-6
+    assert abs(r["E"] - case["total_energy"]) <= 2.5e-7    # measured: 1.6e-7, 5.5e-8, 1.6e-7
 
 
 def test_fock_symmetric_and_linear():

@@ -55,7 +55,7 @@ def test_rhf_energy_golden_h2o_631gs():
     b = build_basis(water(), "6-31G*")
     r = RHF(b, integral_cutoff=1e-11).run(denserms=1e-8)
     assert r["converged"]
-    assert abs(r["E"] - (-75.983996360)) <= 1e-6
+    assert abs(r["E"] - (-75.983996360)) <= 2e-7        # the oracle measures 1.6e-8
 
 
 def test_rhf_matches_oracle_w4_sto3g():
@@ -83,4 +83,5 @@ def test_rhf_golden_nma_def2tzvp_f_shells():
     assert b.has_f
     r = RHF(b, integral_cutoff=1e-11).run(denserms=1e-8)
     assert r["converged"]
+    print(f"NMA/def2-TZVP: E - E_golden = {r['E'] - case['total_energy']:.3e}")
     assert abs(r["E"] - case["total_energy"]) <= 2e-6, (r["E"], case["total_energy"])
