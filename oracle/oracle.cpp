@@ -251,6 +251,12 @@ struct Ctx {
     const double* cutmatrix;  // nshell^2
     const double* cutprim;    // jbasis^2
     double integralCutoff, primLimit;
+    // QUICK's GPU path screens two more things than the CPU get2e: only shell
+    // pairs with Y > 1e-10 enter its pair list (src/gpu/cuda/gpu.cu:929-1030) and
+    // integrals with |Y| <= integralCutoff are not digested
+    // (src/gpu/gpu_get2e_subs.h:389).  gpu_screens reproduces both, to compare
+    // with that implementation; off, this is the CPU get2e.
+    bool gpu_screens = false;
 };
 
 inline double& O(double* G, int n, int r, int c) { return G[(size_t)(r - 1) + (size_t)n * (c - 1)]; }
@@ -379,6 +385,7 @@ void cshell_quartet(const Ctx& C, Work& W, int II, int JJ, int KK, int LL, doubl
                                 for (int KKK = KKK1; KKK <= KKK2; ++KKK)
                                     for (int LLL = LLL1; LLL <= LLL2; ++LLL) {
                                         double Y = hrrwhole(III, JJJ, KKK, LLL);
+                                        if (C.gpu_screens && !(std::fabs(Y) > C.integralCutoff)) continue;
                                         double DKI = Dn(D, n, KKK, III), DKJ = Dn(D, n, KKK, JJJ);
                                         double DLJ = Dn(D, n, LLL, JJJ), DLI = Dn(D, n, LLL, III);
                                         double DLK = Dn(D, n, LLL, KKK), DJI = Dn(D, n, JJJ, III);
@@ -398,6 +405,7 @@ void cshell_quartet(const Ctx& C, Work& W, int II, int JJ, int KK, int LL, doubl
                                     for (int LLL = std::max(KKK, LLL1); LLL <= LLL2; ++LLL) {
                                         if (III < KKK) {
                                             double Y = hrrwhole(III, JJJ, KKK, LLL);
+                                            if (C.gpu_screens && !(std::fabs(Y) > C.integralCutoff)) continue;
                                             if (III < JJJ && KKK < LLL) {
                                                 double DKI = Dn(D, n, KKK, III), DKJ = Dn(D, n, KKK, JJJ);
                                                 double DLJ = Dn(D, n, LLL, JJJ), DLI = Dn(D, n, LLL, III);
@@ -437,6 +445,7 @@ void cshell_quartet(const Ctx& C, Work& W, int II, int JJ, int KK, int LL, doubl
                                             }
                                         } else if (JJJ <= LLL) {
                                             double Y = hrrwhole(III, JJJ, KKK, LLL);
+                                            if (C.gpu_screens && !(std::fabs(Y) > C.integralCutoff)) continue;
                                             if (III == JJJ && III == KKK && III == LLL) {
                                                 double DII = Dn(D, n, III, III);
                                                 O(Gm, n, III, III) += DII * Y - hx * 0.5 * DII * Y;
@@ -705,13 +714,15 @@ void orc_density_cutoff(void* hv, const double* dense, double* cutmatrix) {
 // OpenMP default.
 long long orc_get2e(void* hv, const double* dense, const double* cutmatrix, const double* Ycutoff,
                     const double* cutprim, double integralCutoff, double primLimit, double* o,
-                    int ii_begin, int ii_end, int nthreads, int ii_stride) {
+                    int ii_begin, int ii_end, int nthreads, int ii_stride, int gpu_screens) {
     Basis& B = ((OracleHandle*)hv)->B;
     int n = B.nbasis, ns = B.nshell;
     if (ii_end <= 0 || ii_end > ns) ii_end = ns;
     if (ii_stride <= 0) ii_stride = 1;
     const int nII = (ii_end - ii_begin + ii_stride - 1) / ii_stride;
     Ctx C{&B, dense, cutmatrix, cutprim, integralCutoff, primLimit};
+    C.gpu_screens = gpu_screens != 0;
+    const double pair_cut = C.gpu_screens ? 1e-10 : -1.0;
     std::vector<double> G((size_t)n * n, 0.0);
     long long nq = 0;
 #ifdef _OPENMP
@@ -726,8 +737,10 @@ long long orc_get2e(void* hv, const double* dense, const double* cutmatrix, cons
             const int II = ii_begin + t * ii_stride;
             for (int JJ = II; JJ < ns; ++JJ) {
                 double t = Ycutoff[II + (size_t)ns * JJ];
+                if (!(t > pair_cut)) continue;
                 for (int KK = II; KK < ns; ++KK)
                     for (int LL = KK; LL < ns; ++LL) {
+                        if (!(Ycutoff[KK + (size_t)ns * LL] > pair_cut)) continue;
                         double ct = t * Ycutoff[KK + (size_t)ns * LL];
                         if (!(ct > integralCutoff)) continue;
                         double dnmax = dnmax_of(C, II, JJ, KK, LL);

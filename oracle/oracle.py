@@ -67,7 +67,7 @@ def lib():
         L.orc_schwarz.argtypes = [P, P, P, I]
         L.orc_density_cutoff.argtypes = [P, P, P]
         L.orc_get2e.restype = ctypes.c_longlong
-        L.orc_get2e.argtypes = [P, P, P, P, P, D, D, P, I, I, I, I]
+        L.orc_get2e.argtypes = [P, P, P, P, P, D, D, P, I, I, I, I, I]
         L.orc_oei.argtypes = [I, I, P, P, P, P, P, P, I, P, P, P, P, P]
         _lib = L
     return _lib
@@ -128,14 +128,19 @@ class Oracle:
         return cm
 
     def get2e(self, D, cutmatrix, Ycut, cutprim, integral_cutoff, prim_limit, o=None,
-              ii_range=(0, 0), nthreads=0, ii_stride=1):
-        """Return ``o + G(D)`` (symmetric, nbasis x nbasis) and the quartet count."""
+              ii_range=(0, 0), nthreads=0, ii_stride=1, gpu_screens=False):
+        """Return ``o + G(D)`` (symmetric, nbasis x nbasis) and the quartet count.
+
+        ``gpu_screens``: also apply the two screens of QUICK's GPU path (shell pairs
+        with Y <= 1e-10 left out, integrals with |Y| <= integral_cutoff not
+        digested), to compare with that implementation."""
         b = self.b
         D = _f64(D)
         out = np.zeros((b.nbasis, b.nbasis), order="F") if o is None else _f64(o).copy(order="F")
         nq = lib().orc_get2e(self.h, _p(D), _p(_f64(cutmatrix)), _p(_f64(Ycut)), _p(_f64(cutprim)),
                              float(integral_cutoff), float(prim_limit), _p(out),
-                             int(ii_range[0]), int(ii_range[1]), int(nthreads), int(ii_stride))
+                             int(ii_range[0]), int(ii_range[1]), int(nthreads), int(ii_stride),
+                             int(bool(gpu_screens)))
         return out, nq
 
 

@@ -4,12 +4,12 @@ The reference reads ``basis/<NAME>.BAS`` at run time (``src/basis.f90:65-120``:
 an element header ``"<Sym>  0"``, then shell headers ``"<S|P|SP|D|F> nprim 1.00"``
 each followed by ``nprim`` rows of ``exponent coeff [coeff_p]``, then ``****``).
 These files are Basis Set Exchange data.  This script turns the subset of basis
-sets and elements this package needs into ``<NAME>.json`` beside it, so that the
-package never reads the reference tree at run time.
+sets and elements this package needs into ``quick_b200/basis_data/<NAME>.json``,
+so that the package never reads the reference tree at run time.
 
 Usage (in a checkout that has the reference mounted)::
 
-    python quick_b200/basis_data/extract_basis.py /path/to/QUICK/basis
+    python tests/golden/extract_basis.py /path/to/QUICK/basis
 """
 import json
 import os
@@ -76,5 +76,7 @@ def main(src_dir, dst_dir):
 
 
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis"
-    main(src, os.path.dirname(os.path.abspath(__file__)))
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: extract_basis.py <QUICK source tree>/basis")
+    here = os.path.dirname(os.path.abspath(__file__))
+    main(sys.argv[1], os.path.join(os.path.dirname(os.path.dirname(here)), "quick_b200", "basis_data"))

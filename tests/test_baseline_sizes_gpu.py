@@ -133,20 +133,29 @@ def _refgpu():
 
 @pytest.mark.parametrize("name", ["w4", "w32"])
 def test_reference_gpu_get2e_matches_oracle_and_ours(name):
-    """QUICK's GPU path keeps only shell pairs with Y > 1e-10 (src/gpu/cuda/gpu.cu:929-1030)
-    and drops integrals below integralCutoff (src/gpu/gpu_get2e_subs.h:389); at cutoff
-    1e-10 those screens change G by far less than the parity tolerance."""
+    """QUICK's own GPU get2e against the oracle run with that path's two extra
+    screens (shell pairs with Y > 1e-10 only, src/gpu/cuda/gpu.cu:929-1030;
+    integrals with |Y| <= integralCutoff not digested, src/gpu/gpu_get2e_subs.h:389):
+    max |dG| <= 1e-9, an independent check of the oracle's Boys function, VRR and
+    HRR against the reference's own device code.  Against the plain oracle (the
+    CPU get2e's screens, which this library follows) the difference is those
+    screens' contribution, measured 5e-8 (4 H2O) and 2.3e-6 (32 H2O) at cutoff
+    1e-10."""
     _cuda()
     refgpu = _refgpu()
     b, orc, (Y, cp) = _setup(name)
     D = _core_density(b)
     cm = orc.density_cutoff(D)
     G_orc, _ = orc.get2e(D, cm, Y, cp, CUT, PRIM)
+    G_orc_gs, _ = orc.get2e(D, cm, Y, cp, CUT, PRIM, gpu_screens=True)
     G_ref, info = refgpu.run(b, D, cm, Y, cp, CUT, PRIM, steps=2, warmup=1)
     G = _gpu_fock(b, D, Y, cp)
-    e_ref_orc = float(np.abs(G_ref - G_orc).max())
-    e_ours_ref = float(np.abs(G - G_ref).max())
-    print(f"{name}: |G_refgpu - G_oracle| = {e_ref_orc:.3e}, |G_ours - G_refgpu| = {e_ours_ref:.3e}, {info}")
+    e_gs = float(np.abs(G_ref - G_orc_gs).max())
+    e_plain = float(np.abs(G_ref - G_orc).max())
+    e_ours = float(np.abs(G - G_orc).max())
+    print(f"{name}: |G_refgpu - G_oracle(gpu screens)| = {e_gs:.3e}, |G_refgpu - G_oracle| = {e_plain:.3e}, "
+          f"|G_ours - G_oracle| = {e_ours:.3e}, {info}")
     assert info["bit_identical_repeat"]
-    assert e_ref_orc <= FOCK_TOL, e_ref_orc
-    assert e_ours_ref <= FOCK_TOL, e_ours_ref
+    assert e_gs <= FOCK_TOL, e_gs
+    assert e_plain <= 5e-6, e_plain
+    assert e_ours <= FOCK_TOL, e_ours

@@ -83,5 +83,5 @@ def test_rhf_golden_nma_def2tzvp_f_shells():
     assert b.has_f
     r = RHF(b, integral_cutoff=1e-11).run(denserms=1e-8)
     assert r["converged"]
-    print(f"NMA/def2-TZVP: E - E_golden = {r['E'] - case['total_energy']:.3e}")
-    assert abs(r["E"] - case["total_energy"]) <= 2e-6, (r["E"], case["total_energy"])
+    # measured -5.2e-7 Eh (the golden is the reference CPU build's, 9 decimals)
+    assert abs(r["E"] - case["total_energy"]) <= 6e-7, (r["E"], case["total_energy"])
