@@ -18,10 +18,12 @@
 //   vertical + PSSS..       src/subs/hrr.f90:1051-3456, src/subs/spdfgh.f90
 //                           (HGP eq. 6 written as one generic recursion)
 //   copySym                 src/subs/copySym.f90:16-27
-// Deviation: the Boys function F_m(T) is evaluated with a Taylor expansion on
-// a tabulated grid (table filled from the convergent series) instead of the
-// fitted polynomials of src/subs/fmt.f90; both are accurate to ~1e-14
-// relative, far inside the 1e-9 Fock tolerance.
+// Boys function: by default F_m(T) is evaluated accurately, with a Taylor
+// expansion on a tabulated grid (table filled from the convergent series).
+// src/subs/fmt.f90's fitted polynomials agree with it to ~1e-12 except in its
+// small-X branch, F_M = (1 - X)/(2M + 1) for X <= 0.1 (M >= 4) or X <= 1e-4,
+// which is first order in X; orc_set_boys_mode(1) switches to a restatement of
+// fmt.f90 (boys_quick) to reproduce the reference's own numbers.
 //
 // One-electron integrals (overlap, kinetic, nuclear attraction) follow the
 // Obara-Saika recursions over the normalize_basis representation
@@ -89,8 +91,76 @@ void init_boys() {
             g_boys_tab[i][m] = (double)boys_series(m, (long double)(i * BOYS_DT));
 }
 
+// F_0..F_M at T as QUICK computes it (src/subs/fmt.f90:13-85; the device copy,
+// src/gpu/gpu_fmt.h:5-72, has the same branches): fitted polynomials in 1/X
+// above X = 5, polynomials around X = 2 and 4 on (1, 5], a series-derived
+// polynomial on (0.1, 1] (down to 1e-4 when M < 4), and below that
+// F_M = (1 - X)/(2M + 1), followed by upward or downward recursion.  The last
+// branch is first order in X (relative error up to ~2% in F_M at X = 0.1, M = 4),
+// so the reference's integrals differ from exact ones there.
+void boys_quick(int M, double X, double* F) {
+    const double PIE4 = PI / 4.0;
+    const double XINV = 1.0 / X;
+    const double E = std::exp(-X);
+    double WW1;
+    if (X > 5.0) {
+        if (X > 15.0) {
+            if (X > 33.0)
+                WW1 = std::sqrt(PIE4 * XINV);
+            else
+                WW1 = ((1.9623264149430e-01 * XINV - 4.9695241464490e-01) * XINV - 6.0156581186481e-05) * E +
+                      std::sqrt(PIE4 * XINV);
+        } else if (X > 10.0) {
+            WW1 = (((-1.8784686463512e-01 * XINV + 2.2991849164985e-01) * XINV - 4.9893752514047e-01) * XINV -
+                   2.1916512131607e-05) * E + std::sqrt(PIE4 * XINV);
+        } else {
+            WW1 = ((((((4.6897511375022e-01 * XINV - 6.9955602298985e-01) * XINV + 5.3689283271887e-01) * XINV -
+                      3.2883030418398e-01) * XINV + 2.4645596956002e-01) * XINV - 4.9984072848436e-01) * XINV -
+                   3.1501078774085e-06) * E + std::sqrt(PIE4 * XINV);
+        }
+    } else if (X > 1.0) {
+        double F1;
+        if (X > 3.0) {
+            const double Y = X - 4.0;
+            F1 = ((((((((((-2.62453564772299e-11 * Y + 3.24031041623823e-10) * Y - 3.614965656163e-09) * Y +
+                         3.760256799971e-08) * Y - 3.553558319675e-07) * Y + 3.022556449731e-06) * Y -
+                      2.290098979647e-05) * Y + 1.526537461148e-04) * Y - 8.81947375894379e-04) * Y +
+                   4.33207949514611e-03) * Y - 1.75257821619926e-02) * Y + 5.28406320615584e-02;
+        } else {
+            const double Y = X - 2.0;
+            F1 = ((((((((((-1.61702782425558e-10 * Y + 1.96215250865776e-09) * Y - 2.14234468198419e-08) * Y +
+                         2.17216556336318e-07) * Y - 1.98850171329371e-06) * Y + 1.62429321438911e-05) * Y -
+                      1.16740298039895e-04) * Y + 7.24888732052332e-04) * Y - 3.79490003707156e-03) * Y +
+                   1.61723488664661e-02) * Y - 5.29428148329736e-02) * Y + 1.15702180856167e-01;
+        }
+        WW1 = (X + X) * F1 + E;
+    } else if (X > 1.0e-1 || (X > 1.0e-4 && M < 4)) {
+        const double F1 = ((((((((-8.36313918003957e-08 * X + 1.21222603512827e-06) * X - 1.15662609053481e-05) * X +
+                                9.25197374512647e-05) * X - 6.40994113129432e-04) * X + 3.78787044215009e-03) * X -
+                             1.85185172458485e-02) * X + 7.14285713298222e-02) * X - 1.99999999997023e-01) * X +
+                          3.33333333333318e-01;
+        WW1 = (X + X) * F1 + E;
+    } else {
+        WW1 = (1.0 - X) / (double)(2 * M + 1);
+    }
+    if (X > 1.0e-1 || (X > 1.0e-4 && M < 4)) {
+        F[0] = WW1;
+        for (int m = 1; m <= M; ++m) F[m] = (((2 * m - 1) * F[m - 1]) - E) * 0.5 * XINV;
+    } else {
+        F[M] = WW1;
+        const double twot = X * 2.0;
+        for (int m = M - 1; m >= 0; --m) F[m] = (twot * F[m + 1] + E) / (double)(m * 2 + 1);
+    }
+}
+
+// Boys function used by the integral code: 0 = accurate (the tabulated Taylor
+// form below), 1 = QUICK's own (boys_quick), to compare with the reference's
+// implementations at the last digits.
+int g_boys_mode = 0;
+
 // F_0..F_M at T
 void boys(int M, double T, double* F) {
+    if (g_boys_mode == 1) { boys_quick(M, T, F); return; }
     if (T < 36.0) {
         int k = (int)(T / BOYS_DT + 0.5);
         double d = T - k * BOYS_DT;
@@ -668,6 +738,14 @@ void* orc_create(int natom, const double* xyz, int nshell, int nbasis, int jbasi
 }
 
 void orc_destroy(void* h) { delete (OracleHandle*)h; }
+
+// Select the Boys function of the integral code (0 accurate, 1 QUICK's fmt.f90);
+// returns the previous mode.  Process-wide: set it before a build, not during one.
+int orc_set_boys_mode(int mode) {
+    const int old = g_boys_mode;
+    g_boys_mode = mode ? 1 : 0;
+    return old;
+}
 
 void orc_boys(int M, double T, double* F) {
     static bool inited = false;

@@ -64,6 +64,8 @@ def lib():
         L.orc_create.argtypes = [I, P, I, I, I] + [P] * 13
         L.orc_destroy.argtypes = [P]
         L.orc_boys.argtypes = [I, D, P]
+        L.orc_set_boys_mode.argtypes = [I]
+        L.orc_set_boys_mode.restype = I
         L.orc_schwarz.argtypes = [P, P, P, I]
         L.orc_density_cutoff.argtypes = [P, P, P]
         L.orc_get2e.restype = ctypes.c_longlong
@@ -83,6 +85,20 @@ def _f64(a):
 
 def _i32(a):
     return np.asfortranarray(a, dtype=np.int32)
+
+
+class quick_boys:
+    """Context manager: the oracle's integrals use QUICK's own Boys function
+    (a restatement of src/subs/fmt.f90, first order in X below X = 0.1) instead of
+    the accurate one, to reproduce the reference's numbers to the last digits."""
+
+    def __enter__(self):
+        self.old = lib().orc_set_boys_mode(1)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_boys_mode(self.old)
+        return False
 
 
 def boys(M: int, T: float) -> np.ndarray:

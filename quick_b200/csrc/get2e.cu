@@ -55,16 +55,14 @@ struct DevData {
     const int* __restrict__ pr_npp;
     const int* __restrict__ pr_pps;      // stride between a pair's primitive pairs
     const double* __restrict__ pr_Y;
-    const double* __restrict__ pp_zeta;  // per primitive pair
-    const double* __restrict__ pp_oo2z;
-    const double* __restrict__ pp_K;
-    const double* __restrict__ pp_cut;
-    const double* __restrict__ pp_Px;    // P, and P - centre of the first shell
-    const double* __restrict__ pp_Py;
-    const double* __restrict__ pp_Pz;
-    const double* __restrict__ pp_PAx;
-    const double* __restrict__ pp_PAy;
-    const double* __restrict__ pp_PAz;
+    // per primitive pair, five 16-byte fields (one vector load each):
+    // (zeta, 1/(2 zeta)), (K, cutprim), (Px, Py), (Pz, PAx), (PAy, PAz) with
+    // K = exp(-ab/zeta R_AB^2)/zeta c_a c_b sqrt(X0) and PA = P - centre of the first shell
+    const double2* __restrict__ pp_zo;
+    const double2* __restrict__ pp_kc;
+    const double2* __restrict__ pp_pxy;
+    const double2* __restrict__ pp_pzax;
+    const double2* __restrict__ pp_payz;
     const double* __restrict__ boys;     // kBoysNT x kBoysNM
     const double2* __restrict__ boys8;   // row tables, M = 0..4 kMaxL (boys_row_tables)
     const double* __restrict__ D;        // nbasis^2
@@ -104,21 +102,21 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, const double2
     // the same for the whole warp
     for (int j = 0; j < knp; ++j) {
         const int pj = kp0 + j * kps;
-        const double cutj = __ldg(d.pp_cut + pj);
-        const double eta = __ldg(d.pp_zeta + pj);
-        const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
-        const double Kcd = __ldg(d.pp_K + pj);
-        const double oo2e = __ldg(d.pp_oo2z + pj);
+        const double2 kcj = __ldg(d.pp_kc + pj), zoj = __ldg(d.pp_zo + pj);
+        const double2 qxy = __ldg(d.pp_pxy + pj), qzax = __ldg(d.pp_pzax + pj);
+        const double cutj = kcj.y, eta = zoj.x, oo2e = zoj.y, Kcd = kcj.x;
+        const double Qx = qxy.x, Qy = qxy.y, Qz = qzax.x;
         for (int i = 0; i < bnp; ++i) {
             const int pi = bp0 + i * bps;
-            const double cut1 = dnmax * __ldg(d.pp_cut + pi);
+            const double2 kci = __ldg(d.pp_kc + pi);
+            const double cut1 = dnmax * kci.y;
             if (prim_screen && !(cut1 * cutj > d.primLimit)) continue;
             ++*nprim_done;
-            const double zeta = __ldg(d.pp_zeta + pi);
-            const double oo2z = __ldg(d.pp_oo2z + pi);
-            const double Kab = __ldg(d.pp_K + pi) * kX0;
-            const double Px = __ldg(d.pp_Px + pi), Py = __ldg(d.pp_Py + pi), Pz = __ldg(d.pp_Pz + pi);
-            const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
+            const double2 zoi = __ldg(d.pp_zo + pi), pxy = __ldg(d.pp_pxy + pi);
+            const double2 pzax = __ldg(d.pp_pzax + pi), payz = __ldg(d.pp_payz + pi);
+            const double zeta = zoi.x, oo2z = zoi.y, Kab = kci.x;
+            const double Px = pxy.x, Py = pxy.y, Pz = pzax.x;
+            const double PAx = pzax.y, PAy = payz.x, PAz = payz.y;
             const double s = zeta + eta;
             const double rs = rsqrt(s);            // 1/sqrt(zeta+eta), 1 ulp
             const double inv_s = rs * rs;
@@ -347,22 +345,25 @@ __device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp
     double* gs = acc + Lay::PER_WARP - Lay::GEO;          // this warp's geometry table
     for (int i = 0; i < bnp; ++i) {
         const int pi = bp0 + i * bps;
-        const double zeta = __ldg(d.pp_zeta + pi), oo2z = __ldg(d.pp_oo2z + pi);
-        const double Kab = __ldg(d.pp_K + pi) * kX0;
-        const double cut1 = dnmax * __ldg(d.pp_cut + pi);
-        const double Px = __ldg(d.pp_Px + pi), Py = __ldg(d.pp_Py + pi), Pz = __ldg(d.pp_Pz + pi);
-        const double PAx = __ldg(d.pp_PAx + pi), PAy = __ldg(d.pp_PAy + pi), PAz = __ldg(d.pp_PAz + pi);
+        const double2 zoi = __ldg(d.pp_zo + pi), kci = __ldg(d.pp_kc + pi), pxy = __ldg(d.pp_pxy + pi);
+        const double2 pzax = __ldg(d.pp_pzax + pi), payz = __ldg(d.pp_payz + pi);
+        const double zeta = zoi.x, oo2z = zoi.y, Kab = kci.x;
+        const double cut1 = dnmax * kci.y;
+        const double Px = pxy.x, Py = pxy.y, Pz = pzax.x;
+        const double PAx = pzax.y, PAy = payz.x, PAz = payz.y;
         for (int j = 0; j < knp; ++j) {
             const int pj = kp0 + j * kps;
-            if (screen && !(cut1 * __ldg(d.pp_cut + pj) > d.primLimit)) continue;   // warp-uniform
+            const double2 kcj = __ldg(d.pp_kc + pj);
+            if (screen && !(cut1 * kcj.y > d.primLimit)) continue;   // warp-uniform
             if (lane == 0) ++*np_done;
-            const double eta = __ldg(d.pp_zeta + pj), oo2e = __ldg(d.pp_oo2z + pj);
-            const double Qx = __ldg(d.pp_Px + pj), Qy = __ldg(d.pp_Py + pj), Qz = __ldg(d.pp_Pz + pj);
+            const double2 zoj = __ldg(d.pp_zo + pj), qxy = __ldg(d.pp_pxy + pj), qzax = __ldg(d.pp_pzax + pj);
+            const double eta = zoj.x, oo2e = zoj.y;
+            const double Qx = qxy.x, Qy = qxy.y, Qz = qzax.x;
             const double s = zeta + eta, rs = rsqrt(s), inv_s = rs * rs;
             const double rho_z = eta * inv_s, rho_e = zeta * inv_s, rho = zeta * rho_z;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = Kab * __ldg(d.pp_K + pj) * rs;
+            const double pref = Kab * kcj.x * rs;
             if (lane <= M) V[lane] = boys_one(lane, T, d.boys) * pref;
             if (lane == 0) {
                 gs[0] = PAx; gs[1] = PAy; gs[2] = PAz;
@@ -965,14 +966,14 @@ struct Bucket {
 struct PairTable {
     std::vector<int> qa, qb, pp0, npp, pps;
     std::vector<double> Y;
-    std::vector<double> zeta, oo2z, K, cut, Px, Py, Pz, PAx, PAy, PAz;
+    std::vector<double2> zo, kc, pxy, pzax, payz;   // the five 16-byte fields of DevData
     std::vector<Bucket> buckets;
     DevBuf<int> d_qa, d_qb, d_pp0, d_npp, d_pps;
-    DevBuf<double> d_Y, d_zeta, d_oo2z, d_K, d_cut, d_Px, d_Py, d_Pz, d_PAx, d_PAy, d_PAz;
+    DevBuf<double> d_Y;
+    DevBuf<double2> d_zo, d_kc, d_pxy, d_pzax, d_payz;
     void clear() {
         qa.clear(); qb.clear(); pp0.clear(); npp.clear(); pps.clear(); Y.clear();
-        zeta.clear(); oo2z.clear(); K.clear(); cut.clear();
-        Px.clear(); Py.clear(); Pz.clear(); PAx.clear(); PAy.clear(); PAz.clear(); buckets.clear();
+        zo.clear(); kc.clear(); pxy.clear(); pzax.clear(); payz.clear(); buckets.clear();
     }
 };
 
@@ -1175,16 +1176,11 @@ static DevData make_devdata(qk_ctx* c) {
     d.pr_npp = c->pairs.d_npp.p;
     d.pr_pps = c->pairs.d_pps.p;
     d.pr_Y = c->pairs.d_Y.p;
-    d.pp_zeta = c->pairs.d_zeta.p;
-    d.pp_oo2z = c->pairs.d_oo2z.p;
-    d.pp_K = c->pairs.d_K.p;
-    d.pp_cut = c->pairs.d_cut.p;
-    d.pp_Px = c->pairs.d_Px.p;
-    d.pp_Py = c->pairs.d_Py.p;
-    d.pp_Pz = c->pairs.d_Pz.p;
-    d.pp_PAx = c->pairs.d_PAx.p;
-    d.pp_PAy = c->pairs.d_PAy.p;
-    d.pp_PAz = c->pairs.d_PAz.p;
+    d.pp_zo = c->pairs.d_zo.p;
+    d.pp_kc = c->pairs.d_kc.p;
+    d.pp_pxy = c->pairs.d_pxy.p;
+    d.pp_pzax = c->pairs.d_pzax.p;
+    d.pp_payz = c->pairs.d_payz.p;
     d.boys = c->d_boys.p;
     d.boys8 = (const double2*)c->d_boys8.p;
     d.cut = c->integralCutoff;
@@ -1258,9 +1254,10 @@ static void build_pairs(qk_ctx* c, bool screened) {
             total += T.npp[P];
         }
     }
-    T.zeta.assign(total, 0.0); T.oo2z.assign(total, 0.0); T.K.assign(total, 0.0); T.cut.assign(total, 0.0);
-    T.Px.assign(total, 0.0); T.Py.assign(total, 0.0); T.Pz.assign(total, 0.0);
-    T.PAx.assign(total, 0.0); T.PAy.assign(total, 0.0); T.PAz.assign(total, 0.0);
+    const double2 zero2 = make_double2(0.0, 0.0);
+    T.zo.assign(total, zero2); T.kc.assign(total, zero2); T.pxy.assign(total, zero2);
+    T.pzax.assign(total, zero2); T.payz.assign(total, zero2);
+    const double sqrtX0 = std::sqrt(kX0);
     for (int P = 0; P < np; ++P) {
         const Qsh &a = c->qsh[T.qa[P]], &b = c->qsh[T.qb[P]];
         const double* A = &c->xyz[3 * a.atom];
@@ -1271,14 +1268,17 @@ static void build_pairs(qk_ctx* c, bool screened) {
                 const size_t at = (size_t)T.pp0[P] + (size_t)(i * b.nprim + j) * T.pps[P];
                 const double ea = a.expo[i], eb = b.expo[j], z = ea + eb;
                 // Xcoeff without X0 (src/modules/include/eri.fh:118-140)
-                T.K[at] = std::exp(-ea * eb / z * r2) / z * a.coef[i] * b.coef[j];
-                T.cut[at] = screened ? c->cutprim[(size_t)(a.prim0 + i) * c->jbasis + (b.prim0 + j)] : 0.0;
-                T.zeta[at] = z;
-                T.oo2z[at] = 0.5 / z;
+                // Xcoeff without X0 (src/modules/include/eri.fh:118-140) times sqrt(X0): the
+                // product of a bra's and a ket's K carries the whole X0
+                const double K = std::exp(-ea * eb / z * r2) / z * a.coef[i] * b.coef[j] * sqrtX0;
+                const double cut = screened ? c->cutprim[(size_t)(a.prim0 + i) * c->jbasis + (b.prim0 + j)] : 0.0;
+                T.kc[at] = make_double2(K, cut);
+                T.zo[at] = make_double2(z, 0.5 / z);
                 const double px = (A[0] * ea + B[0] * eb) / z, py = (A[1] * ea + B[1] * eb) / z,
                              pz = (A[2] * ea + B[2] * eb) / z;
-                T.Px[at] = px; T.Py[at] = py; T.Pz[at] = pz;
-                T.PAx[at] = px - A[0]; T.PAy[at] = py - A[1]; T.PAz[at] = pz - A[2];
+                T.pxy[at] = make_double2(px, py);
+                T.pzax[at] = make_double2(pz, px - A[0]);
+                T.payz[at] = make_double2(py - A[1], pz - A[2]);
             }
     }
 }
@@ -1292,16 +1292,11 @@ static int upload_pairs(qk_ctx* c) {
     QK_CUDA_TRY(T.d_npp.upload(T.npp, s));
     QK_CUDA_TRY(T.d_pps.upload(T.pps, s));
     QK_CUDA_TRY(T.d_Y.upload(T.Y, s));
-    QK_CUDA_TRY(T.d_zeta.upload(T.zeta, s));
-    QK_CUDA_TRY(T.d_oo2z.upload(T.oo2z, s));
-    QK_CUDA_TRY(T.d_K.upload(T.K, s));
-    QK_CUDA_TRY(T.d_cut.upload(T.cut, s));
-    QK_CUDA_TRY(T.d_Px.upload(T.Px, s));
-    QK_CUDA_TRY(T.d_Py.upload(T.Py, s));
-    QK_CUDA_TRY(T.d_Pz.upload(T.Pz, s));
-    QK_CUDA_TRY(T.d_PAx.upload(T.PAx, s));
-    QK_CUDA_TRY(T.d_PAy.upload(T.PAy, s));
-    QK_CUDA_TRY(T.d_PAz.upload(T.PAz, s));
+    QK_CUDA_TRY(T.d_zo.upload(T.zo, s));
+    QK_CUDA_TRY(T.d_kc.upload(T.kc, s));
+    QK_CUDA_TRY(T.d_pxy.upload(T.pxy, s));
+    QK_CUDA_TRY(T.d_pzax.upload(T.pzax, s));
+    QK_CUDA_TRY(T.d_payz.upload(T.payz, s));
     return QK_OK;
 }
 
@@ -2272,9 +2267,8 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     for (int ci = 0; ci < kNumClasses; ++ci) it += c->work[ci].d_items.bytes();
     unsigned long long t = it;
     for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
-                     T.d_Y.bytes(), T.d_zeta.bytes(), T.d_oo2z.bytes(), T.d_K.bytes(), T.d_cut.bytes(),
-                     T.d_Px.bytes(), T.d_Py.bytes(), T.d_Pz.bytes(), T.d_PAx.bytes(), T.d_PAy.bytes(),
-                     T.d_PAz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
+                     T.d_Y.bytes(), T.d_zo.bytes(), T.d_kc.bytes(), T.d_pxy.bytes(), T.d_pzax.bytes(),
+                     T.d_payz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
                      c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(),
                      c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
                      c->d_A.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
