@@ -514,7 +514,11 @@ def measure(name, args, dev, stream, flush, local, world, pg, full):
                                    "converged": bool(r3["converged"])}
         res["scf"] = scf
 
-    if full and args.reference_gpu:
+    # The baselines leg (headline workload, one rank): the reference implementations
+    # timed beside this one -- the CPU get2e restatement on the host cores and
+    # QUICK's own CUDA get2e on this GPU -- and this run's G against the oracle's.
+    # The only part of the GPU arm that runs anything under oracle/.
+    if full and not args.no_cpu and world == 1 and args.reference_gpu:
         ref = reference_gpu_figures(basis, D_host, steps)
         G_ref = ref.pop("G", None)
         if G_ref is not None:
@@ -611,7 +615,8 @@ def main():
                     help="skip QUICK's own GPU get2e on the headline workload")
     ap.add_argument("--fp32-bound", type=float, default=1e-5,
                     help="mixed form: FP32 below this Schwarz bound product (0 = skip)")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the baselines leg (CPU oracle sample, QUICK's GPU get2e, parity vs the oracle)")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)

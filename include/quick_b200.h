@@ -129,6 +129,16 @@ int qk_set_cutoffs(qk_ctx *ctx, double integralCutoff, double primLimit);
  * digestion and the fixed-point accumulation stay FP64, as do the high angular
  * momentum (cooperative) classes.  0 (the default) = plain FP64. */
 int qk_set_precision(qk_ctx *ctx, double fp32_bound);
+/* Boys function of the integral kernels.  0 (the default): a 7-term Taylor step from a
+ * tabulated grid below T = 36, the asymptotic form above, accurate to ~2e-15 relative for
+ * every order used.  1 and 2: QUICK's own formulas (src/subs/fmt.f90:13-85; device copy
+ * src/gpu/gpu_fmt.h:5-72) operation by operation, to reproduce the reference's Fock
+ * matrices -- including their first-order branch below T = 0.1 and the precision their
+ * upward recursion loses for high orders at small T.  Mode 1 evaluates at the order
+ * QUICK's CPU get2e uses (the shell quartet's, SP shells counting 1: eri.fh:259, 394);
+ * mode 2 at the order of the split s/p class, as QUICK's GPU get2e does
+ * (src/gpu/gpu_get2e_subs.h:266).  Applies to the Fock builds and to qk_schwarz. */
+int qk_set_boys(qk_ctx *ctx, int mode);
 /* Shell quartets of the current work lists that run in FP32 (mixed form). */
 int qk_last_work_mixed(qk_ctx *ctx, long long *quartets_fp32);
 
@@ -246,9 +256,10 @@ int qk_class_profile(qk_ctx *ctx, int max_classes, int *cls, float *ms, long lon
 int qk_fp64_peak(int device, double *gflops);
 /* Diagnostic: the Boys function F_0..F_M (M <= 4 * qk_max_l()) at n points T[i] >= 0
  * (host arrays), evaluated on the device by the two forms the Fock kernels use: the
- * per-lane kernels' row-table Taylor/downward-recursion evaluation (F_rows) and the
- * cooperative kernels' one-m evaluation (F_one); out[i*(M+1) + m].  No counterpart in
- * the reference, whose device Boys is src/gpu/gpu_fmt.h:5-72.  Synchronises. */
+ * per-lane kernels' evaluation of all orders at once (F_rows) and the cooperative
+ * kernels' one-order evaluation (F_one), in the context's qk_set_boys mode;
+ * out[i*(M+1) + m].  No counterpart in the reference, whose device Boys is
+ * src/gpu/gpu_fmt.h:5-72.  Synchronises. */
 int qk_boys(qk_ctx *ctx, int M, const double *T, int n, double *F_rows, double *F_one);
 
 /* Solve the n x n system A x = b (row-major device arrays, n <= 64) on `stream`

@@ -98,58 +98,80 @@ void init_boys() {
 // F_M = (1 - X)/(2M + 1), followed by upward or downward recursion.  The last
 // branch is first order in X (relative error up to ~2% in F_M at X = 0.1, M = 4),
 // so the reference's integrals differ from exact ones there.
+// One multiply or add, rounded on its own (the empty asm keeps the compiler from
+// fusing it with a neighbour into an FMA): boys_quick rounds exactly as the
+// device copy of it does, which uses __dmul_rn / __dadd_rn.
+inline double mul_rn(double a, double b) {
+    double r = a * b;
+    asm volatile("" : "+x"(r));
+    return r;
+}
+inline double add_rn(double a, double b) {
+    double r = a + b;
+    asm volatile("" : "+x"(r));
+    return r;
+}
+// Horner's rule, c[0] the leading coefficient, one rounding per operation
+inline double horner_rn(const double* c, int n, double x) {
+    double p = c[0];
+    for (int i = 1; i < n; ++i) p = add_rn(mul_rn(p, x), c[i]);
+    return p;
+}
+
+// Sensitivity probe: exp(-X) one ulp up inside boys_quick (0 = off).  QUICK's
+// recursion is unstable in parts of its range, so its results depend on the last
+// bit of the exp it links; this shows by how much.
+int g_exp_ulp = 0;
+
 void boys_quick(int M, double X, double* F) {
+    static const double c33[] = {1.9623264149430e-01, -4.9695241464490e-01, -6.0156581186481e-05};
+    static const double c15[] = {-1.8784686463512e-01, 2.2991849164985e-01, -4.9893752514047e-01,
+                                 -2.1916512131607e-05};
+    static const double c10[] = {4.6897511375022e-01, -6.9955602298985e-01, 5.3689283271887e-01,
+                                 -3.2883030418398e-01, 2.4645596956002e-01, -4.9984072848436e-01,
+                                 -3.1501078774085e-06};
+    static const double c4[] = {-2.62453564772299e-11, 3.24031041623823e-10, -3.614965656163e-09,
+                                3.760256799971e-08, -3.553558319675e-07, 3.022556449731e-06,
+                                -2.290098979647e-05, 1.526537461148e-04, -8.81947375894379e-04,
+                                4.33207949514611e-03, -1.75257821619926e-02, 5.28406320615584e-02};
+    static const double c2[] = {-1.61702782425558e-10, 1.96215250865776e-09, -2.14234468198419e-08,
+                                2.17216556336318e-07, -1.98850171329371e-06, 1.62429321438911e-05,
+                                -1.16740298039895e-04, 7.24888732052332e-04, -3.79490003707156e-03,
+                                1.61723488664661e-02, -5.29428148329736e-02, 1.15702180856167e-01};
+    static const double c0[] = {-8.36313918003957e-08, 1.21222603512827e-06, -1.15662609053481e-05,
+                                9.25197374512647e-05, -6.40994113129432e-04, 3.78787044215009e-03,
+                                -1.85185172458485e-02, 7.14285713298222e-02, -1.99999999997023e-01,
+                                3.33333333333318e-01};
     const double PIE4 = PI / 4.0;
     const double XINV = 1.0 / X;
-    const double E = std::exp(-X);
+    const double E = g_exp_ulp ? std::nextafter(std::exp(-X), 2.0) : std::exp(-X);
     double WW1;
     if (X > 5.0) {
-        if (X > 15.0) {
-            if (X > 33.0)
-                WW1 = std::sqrt(PIE4 * XINV);
-            else
-                WW1 = ((1.9623264149430e-01 * XINV - 4.9695241464490e-01) * XINV - 6.0156581186481e-05) * E +
-                      std::sqrt(PIE4 * XINV);
-        } else if (X > 10.0) {
-            WW1 = (((-1.8784686463512e-01 * XINV + 2.2991849164985e-01) * XINV - 4.9893752514047e-01) * XINV -
-                   2.1916512131607e-05) * E + std::sqrt(PIE4 * XINV);
-        } else {
-            WW1 = ((((((4.6897511375022e-01 * XINV - 6.9955602298985e-01) * XINV + 5.3689283271887e-01) * XINV -
-                      3.2883030418398e-01) * XINV + 2.4645596956002e-01) * XINV - 4.9984072848436e-01) * XINV -
-                   3.1501078774085e-06) * E + std::sqrt(PIE4 * XINV);
-        }
+        const double s = std::sqrt(mul_rn(PIE4, XINV));
+        if (X > 33.0)
+            WW1 = s;
+        else if (X > 15.0)
+            WW1 = add_rn(mul_rn(horner_rn(c33, 3, XINV), E), s);
+        else if (X > 10.0)
+            WW1 = add_rn(mul_rn(horner_rn(c15, 4, XINV), E), s);
+        else
+            WW1 = add_rn(mul_rn(horner_rn(c10, 7, XINV), E), s);
     } else if (X > 1.0) {
-        double F1;
-        if (X > 3.0) {
-            const double Y = X - 4.0;
-            F1 = ((((((((((-2.62453564772299e-11 * Y + 3.24031041623823e-10) * Y - 3.614965656163e-09) * Y +
-                         3.760256799971e-08) * Y - 3.553558319675e-07) * Y + 3.022556449731e-06) * Y -
-                      2.290098979647e-05) * Y + 1.526537461148e-04) * Y - 8.81947375894379e-04) * Y +
-                   4.33207949514611e-03) * Y - 1.75257821619926e-02) * Y + 5.28406320615584e-02;
-        } else {
-            const double Y = X - 2.0;
-            F1 = ((((((((((-1.61702782425558e-10 * Y + 1.96215250865776e-09) * Y - 2.14234468198419e-08) * Y +
-                         2.17216556336318e-07) * Y - 1.98850171329371e-06) * Y + 1.62429321438911e-05) * Y -
-                      1.16740298039895e-04) * Y + 7.24888732052332e-04) * Y - 3.79490003707156e-03) * Y +
-                   1.61723488664661e-02) * Y - 5.29428148329736e-02) * Y + 1.15702180856167e-01;
-        }
-        WW1 = (X + X) * F1 + E;
+        const double F1 = X > 3.0 ? horner_rn(c4, 12, add_rn(X, -4.0)) : horner_rn(c2, 12, add_rn(X, -2.0));
+        WW1 = add_rn(mul_rn(add_rn(X, X), F1), E);
     } else if (X > 1.0e-1 || (X > 1.0e-4 && M < 4)) {
-        const double F1 = ((((((((-8.36313918003957e-08 * X + 1.21222603512827e-06) * X - 1.15662609053481e-05) * X +
-                                9.25197374512647e-05) * X - 6.40994113129432e-04) * X + 3.78787044215009e-03) * X -
-                             1.85185172458485e-02) * X + 7.14285713298222e-02) * X - 1.99999999997023e-01) * X +
-                          3.33333333333318e-01;
-        WW1 = (X + X) * F1 + E;
+        WW1 = add_rn(mul_rn(add_rn(X, X), horner_rn(c0, 10, X)), E);
     } else {
-        WW1 = (1.0 - X) / (double)(2 * M + 1);
+        WW1 = add_rn(1.0, -X) / (double)(2 * M + 1);
     }
     if (X > 1.0e-1 || (X > 1.0e-4 && M < 4)) {
         F[0] = WW1;
-        for (int m = 1; m <= M; ++m) F[m] = (((2 * m - 1) * F[m - 1]) - E) * 0.5 * XINV;
+        for (int m = 1; m <= M; ++m)
+            F[m] = mul_rn(mul_rn(add_rn(mul_rn((double)(2 * m - 1), F[m - 1]), -E), 0.5), XINV);
     } else {
         F[M] = WW1;
-        const double twot = X * 2.0;
-        for (int m = M - 1; m >= 0; --m) F[m] = (twot * F[m + 1] + E) / (double)(m * 2 + 1);
+        const double twot = mul_rn(X, 2.0);
+        for (int m = M - 1; m >= 0; --m) F[m] = add_rn(mul_rn(twot, F[m + 1]), E) / (double)(m * 2 + 1);
     }
 }
 
@@ -739,11 +761,13 @@ void* orc_create(int natom, const double* xyz, int nshell, int nbasis, int jbasi
 
 void orc_destroy(void* h) { delete (OracleHandle*)h; }
 
-// Select the Boys function of the integral code (0 accurate, 1 QUICK's fmt.f90);
-// returns the previous mode.  Process-wide: set it before a build, not during one.
+// Select the Boys function of the integral code: bit 0 = QUICK's fmt.f90 (else
+// accurate), bit 1 = its exp(-X) one ulp up (the sensitivity probe); returns the
+// previous mode.  Process-wide: set it before a build, not during one.
 int orc_set_boys_mode(int mode) {
-    const int old = g_boys_mode;
-    g_boys_mode = mode ? 1 : 0;
+    const int old = g_boys_mode | (g_exp_ulp << 1);
+    g_boys_mode = mode & 1;
+    g_exp_ulp = (mode >> 1) & 1;
     return old;
 }
 

@@ -136,6 +136,115 @@ __device__ __forceinline__ void boys_scaled_rows(double T, double scale, const d
     }
 }
 
+// QUICK's own Boys function (src/subs/fmt.f90:13-85; its device copy is
+// src/gpu/gpu_fmt.h:5-72), for the reference-faithful mode (qk_set_boys): fitted
+// polynomials in 1/X above X = 5, polynomials around X = 4 and 2 on (1, 5], a
+// polynomial on (0.1, 1] (down to 1e-4 when M < 4), F_M = (1 - X)/(2M + 1) below,
+// then upward recursion from F_0 or downward from F_M.  It is first order in X
+// below 0.1 and its upward recursion loses precision for large M at small X (at
+// M = 12, X in (0.1, 1) the result is noise), which is why the default mode is
+// the tabulated evaluation above.  Every multiply and add is rounded on its own
+// (__dmul_rn / __dadd_rn: no fused multiply-adds) so that this copy and the
+// oracle's restatement of fmt.f90 round alike.
+__device__ __forceinline__ double qk_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double qk_add(double a, double b) { return __dadd_rn(a, b); }
+template <int N>
+__device__ __forceinline__ double qk_horner(const double (&c)[N], double x) {
+    double p = c[0];
+#pragma unroll
+    for (int i = 1; i < N; ++i) p = qk_add(qk_mul(p, x), c[i]);
+    return p;
+}
+
+struct QuickFmtTop {
+    double ww1, E, XINV;
+    bool up;   // upward recursion from F_0 (else downward from F_M)
+};
+
+__device__ __forceinline__ QuickFmtTop quick_fmt_top(int M, double X) {
+    constexpr double c33[3] = {1.9623264149430e-01, -4.9695241464490e-01, -6.0156581186481e-05};
+    constexpr double c15[4] = {-1.8784686463512e-01, 2.2991849164985e-01, -4.9893752514047e-01,
+                               -2.1916512131607e-05};
+    constexpr double c10[7] = {4.6897511375022e-01, -6.9955602298985e-01, 5.3689283271887e-01,
+                               -3.2883030418398e-01, 2.4645596956002e-01, -4.9984072848436e-01,
+                               -3.1501078774085e-06};
+    constexpr double c4[12] = {-2.62453564772299e-11, 3.24031041623823e-10, -3.614965656163e-09,
+                               3.760256799971e-08, -3.553558319675e-07, 3.022556449731e-06,
+                               -2.290098979647e-05, 1.526537461148e-04, -8.81947375894379e-04,
+                               4.33207949514611e-03, -1.75257821619926e-02, 5.28406320615584e-02};
+    constexpr double c2[12] = {-1.61702782425558e-10, 1.96215250865776e-09, -2.14234468198419e-08,
+                               2.17216556336318e-07, -1.98850171329371e-06, 1.62429321438911e-05,
+                               -1.16740298039895e-04, 7.24888732052332e-04, -3.79490003707156e-03,
+                               1.61723488664661e-02, -5.29428148329736e-02, 1.15702180856167e-01};
+    constexpr double c0[10] = {-8.36313918003957e-08, 1.21222603512827e-06, -1.15662609053481e-05,
+                               9.25197374512647e-05, -6.40994113129432e-04, 3.78787044215009e-03,
+                               -1.85185172458485e-02, 7.14285713298222e-02, -1.99999999997023e-01,
+                               3.33333333333318e-01};
+    constexpr double PIE4 = 3.14159265358979323846264338327950288 / 4.0;
+    QuickFmtTop t;
+    t.XINV = 1.0 / X;
+    t.E = exp(-X);
+    t.up = X > 1.0e-1 || (X > 1.0e-4 && M < 4);
+    if (X > 5.0) {
+        const double s = sqrt(qk_mul(PIE4, t.XINV));
+        if (X > 33.0)
+            t.ww1 = s;
+        else if (X > 15.0)
+            t.ww1 = qk_add(qk_mul(qk_horner(c33, t.XINV), t.E), s);
+        else if (X > 10.0)
+            t.ww1 = qk_add(qk_mul(qk_horner(c15, t.XINV), t.E), s);
+        else
+            t.ww1 = qk_add(qk_mul(qk_horner(c10, t.XINV), t.E), s);
+    } else if (X > 1.0) {
+        const double F1 = X > 3.0 ? qk_horner(c4, qk_add(X, -4.0)) : qk_horner(c2, qk_add(X, -2.0));
+        t.ww1 = qk_add(qk_mul(qk_add(X, X), F1), t.E);
+    } else if (t.up) {
+        t.ww1 = qk_add(qk_mul(qk_add(X, X), qk_horner(c0, X)), t.E);
+    } else {
+        t.ww1 = qk_add(1.0, -X) / (double)(2 * M + 1);
+    }
+    return t;
+}
+
+// F_0..F_M at X by QUICK's formulas evaluated for the order MQ >= M (QUICK's CPU
+// get2e evaluates at the shell quartet's order, which exceeds the class's M when
+// SP shells take part; the branch, and in the downward case the starting value,
+// depend on it), each multiplied by `scale`.
+template <int M>
+__device__ __forceinline__ void boys_quick_scaled(double X, double scale, double* F, int MQ) {
+    const QuickFmtTop t = quick_fmt_top(MQ, X);
+    double G[M + 1];
+    if (t.up) {
+        G[0] = t.ww1;
+#pragma unroll
+        for (int m = 1; m <= M; ++m)
+            G[m] = qk_mul(qk_mul(qk_add(qk_mul((double)(2 * m - 1), G[m - 1]), -t.E), 0.5), t.XINV);
+    } else {
+        const double twot = qk_mul(X, 2.0);
+        double f = t.ww1;
+        for (int m = MQ - 1; m >= M; --m) f = qk_add(qk_mul(twot, f), t.E) / (double)(m * 2 + 1);
+        G[M] = f;
+#pragma unroll
+        for (int m = M - 1; m >= 0; --m) G[m] = qk_add(qk_mul(twot, G[m + 1]), t.E) / (double)(m * 2 + 1);
+    }
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = G[m] * scale;
+}
+
+// F_m at X by QUICK's formulas for a total order M (the recursion runs from F_0
+// up, or from F_M down, to m): one element, for the lane-parallel evaluation.
+__device__ __forceinline__ double boys_quick_one(int m, int M, double X) {
+    const QuickFmtTop t = quick_fmt_top(M, X);
+    double f = t.ww1;
+    if (t.up) {
+        for (int j = 1; j <= m; ++j) f = qk_mul(qk_mul(qk_add(qk_mul((double)(2 * j - 1), f), -t.E), 0.5), t.XINV);
+    } else {
+        const double twot = qk_mul(X, 2.0);
+        for (int j = M - 1; j >= m; --j) f = qk_add(qk_mul(twot, f), t.E) / (double)(j * 2 + 1);
+    }
+    return f;
+}
+
 // Row tables for M = 0 .. 4 kMaxL from boys_table(): block M holds kBoysNT rows
 // of kBoysRow doubles (F_M..F_{M+6}, exp(-T_k)).
 inline std::vector<double> boys_row_tables(const std::vector<double>& tab) {

@@ -49,6 +49,7 @@ struct DevData {
     const int* __restrict__ q_atom;      // per Qshell
     const int* __restrict__ q_f0;
     const int* __restrict__ q_parent;
+    const int* __restrict__ q_ltop;      // per Qshell: the top angular momentum of its shell (1 for SP)
     const int* __restrict__ pr_qa;       // per pair
     const int* __restrict__ pr_qb;
     const int* __restrict__ pr_pp0;
@@ -70,6 +71,7 @@ struct DevData {
     unsigned long long* __restrict__ A;  // nbasis^2 fixed point
     unsigned long long* stats;           // optional: [quartets computed, primitive quartets computed]
     double cut, primLimit;
+    int boys_mode;                       // qk_set_boys: 0 accurate; 1 QUICK CPU order; 2 QUICK GPU order
 };
 
 __device__ __forceinline__ void atomic_fixed(unsigned long long* addr, double v) {
@@ -88,10 +90,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 // the vertical recursion and of acc: double for the plain path, float for the
 // small-bound quartets of the mixed form.  Geometry and the Boys function are
 // always evaluated in FP64 and rounded to R afterwards.
+// mq: the order QUICK's CPU get2e evaluates the Boys function at for this quartet
+// (the sum of the four shells' top angular momenta, SP shells counting 1), used by
+// the QUICK-faithful mode 1 of qk_set_boys.
 template <int La, int Lb, int Lc, int Ld, typename R = double>
 __device__ __forceinline__ void contract_quartet(const DevData& d, const double2* __restrict__ bt, int bp0, int bnp,
                                                  int bps, int kp0, int knp, int kps,
-                                                 const double C[3], double dnmax, bool prim_screen,
+                                                 const double C[3], double dnmax, bool prim_screen, int mq,
                                                  R* acc, int* nprim_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int M = Cls::M;
@@ -126,7 +131,10 @@ __device__ __forceinline__ void contract_quartet(const DevData& d, const double2
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const double pref = Kab * Kcd * rs;
             double F[M + 1];
-            boys_scaled_rows<M>(T, pref, bt, F);
+            if (d.boys_mode)
+                boys_quick_scaled<M>(T, pref, F, d.boys_mode == 1 ? mq : M);
+            else
+                boys_scaled_rows<M>(T, pref, bt, F);
             VrrGeom<R> G;
             G.PA[0] = R(PAx); G.PA[1] = R(PAy); G.PA[2] = R(PAz);
             G.WP[0] = R(-rho_z * PQx); G.WP[1] = R(-rho_z * PQy); G.WP[2] = R(-rho_z * PQz);
@@ -173,17 +181,18 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
     const double Cc[3] = {d.xyz[3 * ic], d.xyz[3 * ic + 1], d.xyz[3 * ic + 2]};
     const double CD[3] = {Cc[0] - d.xyz[3 * id], Cc[1] - d.xyz[3 * id + 1], Cc[2] - d.xyz[3 * id + 2]};
 
+    const int mq = d.q_ltop[qa] + d.q_ltop[qb] + d.q_ltop[qc] + d.q_ltop[qd];
     double acc[NE * NF];
     if constexpr (FP32) {
         // mixed form: small-bound quartet, vertical recursion and contraction in FP32
         float accf[NE * NF];
         contract_quartet<La, Lb, Lc, Ld, float>(d, bt, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q],
-                                                d.pr_npp[Q], d.pr_pps[Q], Cc, dnmax, true, accf, np_done);
+                                                d.pr_npp[Q], d.pr_pps[Q], Cc, dnmax, true, mq, accf, np_done);
 #pragma unroll
         for (int i = 0; i < NE * NF; ++i) acc[i] = (double)accf[i];
     } else {
         contract_quartet<La, Lb, Lc, Ld>(d, bt, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q],
-                                         d.pr_pps[Q], Cc, dnmax, true, acc, np_done);
+                                         d.pr_pps[Q], Cc, dnmax, true, mq, acc, np_done);
     }
 
     // bra HRR per ket column
@@ -334,7 +343,7 @@ struct CoopLayout {
 // level by level over the 32 lanes with its values in V (shared, per warp).
 template <int La, int Lb, int Lc, int Ld>
 __device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp, int bps, int kp0, int knp, int kps,
-                                              double Cx, double Cy, double Cz, double dnmax, bool screen,
+                                              double Cx, double Cy, double Cz, double dnmax, bool screen, int mq,
                                               double* acc, double* V, int lane, int* np_done) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     using Lay = CoopLayout<La, Lb, Lc, Ld>;
@@ -364,7 +373,9 @@ __device__ __forceinline__ void coop_contract(const DevData& d, int bp0, int bnp
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
             const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const double pref = Kab * kcj.x * rs;
-            if (lane <= M) V[lane] = boys_one(lane, T, d.boys) * pref;
+            if (lane <= M)
+                V[lane] = (d.boys_mode ? boys_quick_one(lane, d.boys_mode == 1 ? mq : M, T) : boys_one(lane, T, d.boys)) *
+                          pref;
             if (lane == 0) {
                 gs[0] = PAx; gs[1] = PAy; gs[2] = PAz;
                 gs[3] = Qx - Cx; gs[4] = Qy - Cy; gs[5] = Qz - Cz;
@@ -470,8 +481,9 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     for (int t = lane; t < NA * NC; t += 32) cp_async8(Dac + t, d.D + (size_t)(fa + t / NC) * n + fc + t % NC);
     cp_async_commit();
 
+    const int mq = d.q_ltop[qa] + d.q_ltop[qb] + d.q_ltop[qc] + d.q_ltop[qd];
     coop_contract<La, Lb, Lc, Ld>(d, d.pr_pp0[P], d.pr_npp[P], d.pr_pps[P], d.pr_pp0[Q], d.pr_npp[Q], d.pr_pps[Q],
-                                  Cx, Cy, Cz, dnmax, true, acc, V, lane, np_done);
+                                  Cx, Cy, Cz, dnmax, true, mq, acc, V, lane, np_done);
     __syncwarp();   // acc complete (also when every primitive quartet was screened out)
     // bra HRR (one ket column per lane), then ket HRR (one bra row per lane)
     double* t1 = V;
@@ -740,7 +752,7 @@ schwarz_kernel(DevData d, const int2* __restrict__ work, int n_work, const int* 
     double acc[NE * NF];
     int ndone = 0;
     contract_quartet<La, Lb, La, Lb>(d, d.boys8 + (size_t)Cls::M * kBoysNT * (kBoysRow / 2), p0, np, ps, p0, np, ps,
-                                     Cc, 0.0, false, acc, &ndone);
+                                     Cc, 0.0, false, 2 * (d.q_ltop[qa] + d.q_ltop[qb]), acc, &ndone);
     double t1[NF * NAB];
 #pragma unroll
     for (int f = 0; f < NF; ++f) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, AB[0], AB[1], AB[2]);
@@ -799,7 +811,8 @@ schwarz_coop_kernel(DevData d, const int2* __restrict__ work, int n_work, const 
         if (mode >= 0) { p0 += mode * ps; np = 1; }
         int ndone = 0;
         coop_contract<La, Lb, La, Lb>(d, p0, np, ps, p0, np, ps, d.xyz[3 * ia], d.xyz[3 * ia + 1],
-                                      d.xyz[3 * ia + 2], 0.0, false, acc, V, lane, &ndone);
+                                      d.xyz[3 * ia + 2], 0.0, false, 2 * (d.q_ltop[qa] + d.q_ltop[qb]), acc, V, lane,
+                                      &ndone);
         __syncwarp();
         double* t1 = V;
         double* I = V + NF * NAB;
@@ -887,23 +900,26 @@ __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
 // directly against high-precision values.
 template <int M>
 __global__ void boys_probe_kernel(const double* __restrict__ T, int n, const double2* __restrict__ rows8,
-                                  const double* __restrict__ tab, double* __restrict__ f_rows,
+                                  const double* __restrict__ tab, int mode, double* __restrict__ f_rows,
                                   double* __restrict__ f_one) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double F[M + 1];
-    boys_scaled_rows<M>(T[i], 1.0, rows8 + (size_t)M * kBoysNT * (kBoysRow / 2), F);
+    if (mode)
+        boys_quick_scaled<M>(T[i], 1.0, F, M);
+    else
+        boys_scaled_rows<M>(T[i], 1.0, rows8 + (size_t)M * kBoysNT * (kBoysRow / 2), F);
 #pragma unroll
     for (int m = 0; m <= M; ++m) {
         f_rows[(size_t)i * (M + 1) + m] = F[m];
-        f_one[(size_t)i * (M + 1) + m] = boys_one(m, T[i], tab);
+        f_one[(size_t)i * (M + 1) + m] = mode ? boys_quick_one(m, M, T[i]) : boys_one(m, T[i], tab);
     }
 }
 
 template <int M>
-static cudaError_t launch_boys_probe(const double* T, int n, const double2* rows8, const double* tab, double* fr,
-                                     double* fo, cudaStream_t s) {
-    boys_probe_kernel<M><<<(n + 127) / 128, 128, 0, s>>>(T, n, rows8, tab, fr, fo);
+static cudaError_t launch_boys_probe(const double* T, int n, const double2* rows8, const double* tab, int mode,
+                                     double* fr, double* fo, cudaStream_t s) {
+    boys_probe_kernel<M><<<(n + 127) / 128, 128, 0, s>>>(T, n, rows8, tab, mode, fr, fo);
     return cudaGetLastError();
 }
 
@@ -1077,6 +1093,7 @@ struct qk_ctx {
     std::vector<double> Ycut, cutprim;   // nshell^2, jbasis^2 (symmetric)
     double integralCutoff = 1e-7, primLimit = 1e-8;
     double fp32_bound = 0.0;          // mixed form: FP32 below this Schwarz bound product
+    int boys_mode = 0;                // qk_set_boys: 0 tabulated; 1 QUICK's CPU order; 2 its GPU order
     int nstreams = 4;                 // class kernels run over this many streams (0: one after another)
     int shard_rank = 0, shard_count = 1;   // this context's share of the work items (qk_set_shard)
     int cls_wpb[qk::kNumClasses] = {};    // warps per block of each class launch (0: default)
@@ -1091,7 +1108,7 @@ struct qk_ctx {
     int num_sms = 148;
     // device buffers
     qk::DevBuf<double> d_xyz, d_boys, d_boys8, d_D, d_cutmat, d_o;
-    qk::DevBuf<int> d_q_atom, d_q_f0, d_q_parent, d_q_prim0, d_q_nprim, d_shell_f0, d_shell_f1;
+    qk::DevBuf<int> d_q_atom, d_q_f0, d_q_parent, d_q_ltop, d_q_prim0, d_q_nprim, d_shell_f0, d_shell_f1;
     qk::DevBuf<unsigned long long> d_A;
     qk::DevBuf<int> d_counters;
     // optional per-class timing (CUDA events on the launching stream) and work counters
@@ -1170,6 +1187,7 @@ static DevData make_devdata(qk_ctx* c) {
     d.q_atom = c->d_q_atom.p;
     d.q_f0 = c->d_q_f0.p;
     d.q_parent = c->d_q_parent.p;
+    d.q_ltop = c->d_q_ltop.p;
     d.pr_qa = c->pairs.d_qa.p;
     d.pr_qb = c->pairs.d_qb.p;
     d.pr_pp0 = c->pairs.d_pp0.p;
@@ -1185,6 +1203,7 @@ static DevData make_devdata(qk_ctx* c) {
     d.boys8 = (const double2*)c->d_boys8.p;
     d.cut = c->integralCutoff;
     d.primLimit = c->primLimit;
+    d.boys_mode = c->boys_mode;
     return d;
 }
 
@@ -1843,9 +1862,10 @@ int qk_set_basis(qk_ctx* c, int natom, const double* xyz, int nshell, int nbasis
             c->qsh.push_back(q);
         }
     }
-    std::vector<int> q_atom, q_f0, q_parent, q_prim0, q_nprim;
+    std::vector<int> q_atom, q_f0, q_parent, q_ltop, q_prim0, q_nprim;
     for (auto& q : c->qsh) {
         q_atom.push_back(q.atom); q_f0.push_back(q.f0); q_parent.push_back(q.parent);
+        q_ltop.push_back(Qfinal[q.parent]);
         q_prim0.push_back(q.prim0); q_nprim.push_back(q.nprim);
     }
     cudaStream_t s = c->stream;
@@ -1853,6 +1873,7 @@ int qk_set_basis(qk_ctx* c, int natom, const double* xyz, int nshell, int nbasis
     QK_CUDA_TRY(c->d_q_atom.upload(q_atom, s));
     QK_CUDA_TRY(c->d_q_f0.upload(q_f0, s));
     QK_CUDA_TRY(c->d_q_parent.upload(q_parent, s));
+    QK_CUDA_TRY(c->d_q_ltop.upload(q_ltop, s));
     QK_CUDA_TRY(c->d_q_prim0.upload(q_prim0, s));
     QK_CUDA_TRY(c->d_q_nprim.upload(q_nprim, s));
     QK_CUDA_TRY(c->d_shell_f0.upload(c->shell_f0, s));
@@ -1963,6 +1984,13 @@ int qk_set_precision(qk_ctx* c, double fp32_bound) {
     if (!c || !(fp32_bound >= 0.0)) return fail(QK_ERR_INVALID_ARG, "bad precision bound");
     std::lock_guard<std::mutex> g(c->mu);
     c->fp32_bound = fp32_bound;
+    return QK_OK;
+}
+
+int qk_set_boys(qk_ctx* c, int mode) {
+    if (!c || mode < 0 || mode > 2) return fail(QK_ERR_INVALID_ARG, "qk_set_boys: mode must be 0, 1 or 2");
+    std::lock_guard<std::mutex> g(c->mu);
+    c->boys_mode = mode;
     return QK_OK;
 }
 
@@ -2269,7 +2297,7 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
                      T.d_Y.bytes(), T.d_zo.bytes(), T.d_kc.bytes(), T.d_pxy.bytes(), T.d_pzax.bytes(),
                      T.d_payz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
-                     c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(),
+                     c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(), c->d_q_ltop.bytes(),
                      c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
                      c->d_A.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
         t += b;
@@ -2416,7 +2444,7 @@ int qk_boys(qk_ctx* c, int M, const double* T, int n, double* F_rows, double* F_
     const double* tab = c->d_boys.p;
     cudaError_t e = cudaErrorInvalidValue;
     switch (M) {
-#define QK_BOYS_CASE(m) case m: e = launch_boys_probe<m>(dT.p, n, rows8, tab, dr.p, d1.p, s); break;
+#define QK_BOYS_CASE(m) case m: e = launch_boys_probe<m>(dT.p, n, rows8, tab, c->boys_mode, dr.p, d1.p, s); break;
         QK_BOYS_CASE(0) QK_BOYS_CASE(1) QK_BOYS_CASE(2) QK_BOYS_CASE(3) QK_BOYS_CASE(4)
 #if QK_MAX_L >= 2
         QK_BOYS_CASE(5) QK_BOYS_CASE(6) QK_BOYS_CASE(7) QK_BOYS_CASE(8)

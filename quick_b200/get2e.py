@@ -98,6 +98,12 @@ class Get2e:
         self.fp32_bound = float(fp32_bound)
         check(lib().qk_set_precision(self.h, self.fp32_bound), "qk_set_precision")
 
+    def set_boys(self, mode: int):
+        """Boys function of the integrals: 0 = accurate (default); QUICK's own
+        fmt.f90 formulas at the order its CPU get2e uses (1) or its GPU get2e uses
+        (2), to reproduce the reference's numbers to the last digits."""
+        check(lib().qk_set_boys(self.h, int(mode)), "qk_set_boys")
+
     def fp32_quartets(self):
         q = ctypes.c_longlong(0)
         check(lib().qk_last_work_mixed(self.h, ctypes.byref(q)), "qk_last_work_mixed")

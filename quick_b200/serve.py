@@ -519,6 +519,55 @@ def summarize(results, wall: float) -> dict:
     }
 
 
+def run_sequential(requests, fp32_bound: float = 0.0, device: int = 0, denserms: float = 1e-6,
+                   integral_cutoff: float = 1e-10, maxiter: int = 100):
+    """The plain path the server is measured against: the same requests solved one
+    at a time, in request order, with no batching -- per request its basis, its
+    context (one context rebound to each molecule, as a caller of the one-molecule
+    API would keep it), one-electron integrals with its point charges, the SAD
+    guess (or its series' last density) and a graph-captured SCF (``GraphSCF``).
+    Returns (summary, results); ``solves_per_s`` is the requests over the time
+    to solve all of them back to back, arrivals ignored (the capacity of the
+    plain path)."""
+    import torch
+    from .get2e import Get2e
+    from .scf import RHF, GraphSCF
+    torch.cuda.set_device(device)
+    eng = None
+    series_D = {}
+    results = []
+    t0 = time.perf_counter()
+    for req in requests:
+        ta = time.perf_counter() - t0
+        basis = build_basis(req.mol, req.basis)
+        if eng is None:
+            eng = Get2e(basis, device=device, integral_cutoff=integral_cutoff, prim_limit=0.1 * integral_cutoff)
+            if fp32_bound > 0.0:
+                eng.set_precision(fp32_bound)
+        else:
+            eng.bind(basis)
+        rhf = RHF(basis, device=device, ext_charges=req.ext_charges, engine=eng)
+        D0 = series_D.get(req.series) if req.series is not None else None
+        r = GraphSCF(rhf).run(denserms=denserms, maxiter=maxiter, D0=D0)
+        if req.series is not None and r["converged"]:
+            series_D[req.series] = r["D"]
+        done = time.perf_counter() - t0
+        results.append(Result(req.rid, r["E"], r["niter"], r["converged"], basis.nbasis, req.basis, req.kind,
+                              ta, ta, done, 0, D0 is not None))
+    wall = time.perf_counter() - t0
+    if eng is not None:
+        eng.close()
+    s = summarize(results, wall)
+    s.update({"fp32_bound": fp32_bound, "mode": "sequential: one request at a time, no batching, arrivals "
+                                              "ignored (latency = its own set-up and solve)"})
+    return s, results
+
+
+def _max_dE(results, ref_E):
+    d = [abs(r.E - ref_E[r.rid]) for r in results if r.rid in ref_E]
+    return float(max(d)) if d else None
+
+
 def run_stream(n_requests: int, rate: float, fp32_bound: float = 0.0, seed: int = 20261203,
                memory_budget: int = None, denserms: float = 1e-6, device: int = 0, **stream_kw):
     """Serve one seeded stream; returns (summary dict, results)."""
@@ -559,6 +608,9 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     ap.add_argument("--warmup", type=int, default=64,
                     help="requests served (untimed) first: module loading, SAD atoms, allocator")
+    ap.add_argument("--sequential", action="store_true",
+                    help="also solve the stream one request at a time in plain FP64 (no batching): the baseline "
+                         "of the served forms' solves/s")
     a = ap.parse_args(argv)
     budget = int(a.budget_gb * (1 << 30)) if a.budget_gb else None
     if a.warmup > 0:
@@ -566,6 +618,11 @@ def main(argv=None):
         w.serve(request_stream(a.warmup, 1000.0, seed=a.seed + 1), realtime=False)
         w.close()
     report = []
+    seq = None
+    if a.sequential:
+        seq, rseq = run_sequential(request_stream(a.requests, 1.0, seed=a.seed))
+        print(json.dumps({"sequential_fp64": seq}), flush=True)
+        report.append({"sequential_fp64": seq})
     for rate in a.rate:
         if a.compare:
             s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget)
@@ -574,11 +631,21 @@ def main(argv=None):
             e64 = {r.rid: r.E for r in r64}
             dE = [abs(r.E - e64[r.rid]) for r in r32 if r.rid in e64]
             s32["max_abs_dE_vs_fp64"] = float(max(dE)) if dE else None
+            if seq:
+                e_seq = {r.rid: r.E for r in rseq}
+                s64["max_abs_dE_vs_sequential_fp64"] = _max_dE(r64, e_seq)
+                s32["max_abs_dE_vs_sequential_fp64"] = _max_dE(r32, e_seq)
             line = {"rate_per_s": rate, "fp64": s64, "mixed": s32}
+            if seq:
+                line["mixed_vs_sequential_fp64"] = s32["solves_per_s"] / seq["solves_per_s"]
+                line["fp64_vs_sequential_fp64"] = s64["solves_per_s"] / seq["solves_per_s"]
         else:
-            line, _ = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget)
+            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget)
+            if seq:
+                line["vs_sequential_fp64"] = line["solves_per_s"] / seq["solves_per_s"]
         print(json.dumps(line), flush=True)
         report.append(line)
+
     if a.out:
         with open(a.out, "w") as f:
             json.dump(report, f, indent=1)

@@ -64,3 +64,46 @@ def test_device_boys_against_mpmath(M):
                 worst = max(worst, rel)
                 assert rel <= REL_TOL, (M, m, float(t), got, ref, rel)
     print(f"M={M}: worst relative error {worst:.2e}")
+
+
+@pytest.mark.parametrize("M", [0, 1, 2, 3, 4, 6, 8, 12])
+def test_device_quick_boys_matches_oracle_restatement(M):
+    """The reference-faithful mode (qk_set_boys(1)): the device copy of QUICK's
+    fmt.f90 against the oracle's restatement of it, both rounding every multiply and
+    add on its own.  exp() differs by an ulp between the device and the host
+    library, and QUICK's upward recursion amplifies that by up to ~500 where it is
+    still accurate (M = 4 at T = 0.34: 4e-13 relative) and beyond all digits where
+    it is not (high M at small T); so the two copies must agree to 1e-13 relative
+    plus the error of QUICK's value itself against the exact one."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from oracle import oracle as O
+    from quick_b200._native import check, lib
+    from quick_b200.basis import build_basis
+    from quick_b200.get2e import Get2e
+    from quick_b200.molecules import water_cluster
+    L = lib()
+    if M > 4 * L.qk_max_l():
+        pytest.skip("M above the compiled maximum")
+    eng = Get2e(build_basis(water_cluster(1, 3.0), "STO-3G"))
+    eng.set_boys(1)
+    rng = np.random.default_rng(7)
+    T = np.concatenate([[1e-7, 5e-5, 1e-4, 0.05, 0.1, 0.5, 1.0, 2.0, 3.0, 4.5, 5.0, 7.0, 10.0, 12.0, 15.0, 20.0,
+                         33.0, 40.0, 300.0], np.exp(rng.uniform(np.log(1e-6), np.log(100.0), 60))])
+    n = len(T)
+    Fr, F1 = np.zeros((n, M + 1)), np.zeros((n, M + 1))
+    P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    check(L.qk_boys(ctypes.c_void_p(eng.h), M, P(T), n, P(Fr), P(F1)), "qk_boys")
+    eng.close()
+    tight = 0
+    with O.quick_boys():
+        for i, t in enumerate(T):
+            Fq = O.boys(M, float(t))
+            for m in range(M + 1):
+                exact = _boys_mp(m, float(t))
+                bound = 1e-13 * abs(Fq[m]) + abs(Fq[m] - exact)
+                tight += abs(Fq[m] - exact) <= 1e-13 * abs(exact)
+                for got in (Fr[i, m], F1[i, m]):
+                    assert np.isfinite(got)
+                    assert abs(got - Fq[m]) <= bound, (M, m, float(t), got, Fq[m], exact)
+    assert tight > 0

@@ -196,3 +196,29 @@ def test_linearity_and_symmetry_at_full_size():
     assert err <= 1e-8 * max(1.0, float(G3.abs().max())), err
     assert torch.equal(G3, G3.T)
     eng.close()
+
+
+QUICK_BOYS_CASES = [c for c in CASES if c[0] in ("h2o-631gs", "w3-631gs", "w4-sto3g", "h2o-ccpvtz", "w2-ccpvtz")]
+
+
+@pytest.mark.parametrize("name,molf,bas", QUICK_BOYS_CASES, ids=[c[0] for c in QUICK_BOYS_CASES])
+def test_fock_matches_oracle_with_quick_boys(name, molf, bas, oracle_cache):
+    """Reference-faithful mode: with QUICK's own Boys function on both sides at the
+    order QUICK's CPU get2e evaluates it (qk_set_boys(1); the oracle's restatement
+    of src/subs/fmt.f90) the Fock matrices agree to 1e-9 Eh as in the default mode.
+    The faithful and the default mode differ by fmt.f90's own error (measured
+    1.1e-6 Eh on 32 H2O / 6-31G*)."""
+    _cuda()
+    from quick_b200.get2e import Get2e
+    b, orc, (Y, cp) = _oracle(name, molf(), bas, oracle_cache)
+    D = random_density(b.nbasis)
+    cm = orc.density_cutoff(D)
+    with O.quick_boys():
+        G_ref, _ = orc.get2e(D, cm, Y, cp, 1e-10, 1e-11)
+    eng = Get2e(b, integral_cutoff=1e-10, prim_limit=1e-11, schwarz=(Y, cp))
+    eng.set_boys(1)
+    G = eng.fock2e(torch.tensor(D, device="cuda")).cpu().numpy()
+    eng.close()
+    err = float(np.abs(G - G_ref).max())
+    print(f"{name}: QUICK Boys mode max |dG| = {err:.3e}")
+    assert err <= FOCK_TOL, f"max |dG| = {err:.3e}"
