@@ -226,6 +226,14 @@ int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int
 /* Kernel launches of one build (for launch accounting). */
 int qk_launches_per_build(qk_ctx *ctx);
 
+/* Who builds the work lists (the quartet items each class kernel walks): 1 (the
+ * default) the GPU -- one thread per (bra pair, ket bucket) finds its Schwarz-admitted
+ * ket prefix, scans place the items, two small host synchronisations; 0 the host (the
+ * reference implementation of the lists, also used by sharded contexts).  Both give
+ * the same lists item for item.  The reference builds its pair list on the host
+ * (gpu_upload_cutoff_matrix_, src/gpu/cuda/gpu.cu:879-1470). */
+int qk_set_worklist_builder(qk_ctx *ctx, int on_device);
+
 /* Launch shape of a build: the class kernels run concurrently over `nstreams`
  * auxiliary streams forked from the caller's stream (1..4, default 4), or one after
  * another on the caller's stream (0).  A tuning knob: which is faster depends on

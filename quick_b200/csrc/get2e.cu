@@ -29,11 +29,15 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <tuple>
 #include <vector>
+
+#include <cub/device/device_scan.cuh>
 
 #include "quick_b200.h"
 #include "common.cuh"
@@ -1068,8 +1072,9 @@ static const ClassEntry g_classes[] = {QK_ERI_CLASS_LIST(QK_X)};
 constexpr int kNumClasses = sizeof(g_classes) / sizeof(g_classes[0]);
 
 struct ClassWork {
-    std::vector<int4> items;
-    DevBuf<int4> d_items;
+    std::vector<int4> items;      // host builder only (sharded contexts)
+    const int4* d_items = nullptr;   // this class's items inside the context's item buffer
+    int n_items = 0;
     long long nquart = 0, nprimq = 0, nquart32 = 0;
     int block = 0;        // threads per block of the class launch
     size_t smem = 0;      // dynamic shared memory of a block
@@ -1103,6 +1108,9 @@ struct qk_ctx {
     bool pairs_dirty = true;
     qk::PairTable pairs;
     qk::ClassWork work[qk::kNumClasses];
+    qk::DevBuf<int4> d_items;          // every class's work items, class after class
+    qk::DevBuf<char> d_wl;             // scratch of the device work-list builder
+    bool worklist_on_device = true;    // qk_set_worklist_builder
     int launches = 0;
     long long last_quart = 0, last_primq = 0;
     int num_sms = 148;
@@ -1325,6 +1333,25 @@ static int upload_pairs(qk_ctx* c) {
 // (tuned or default), the matching dynamic shared memory (cooperative classes:
 // one work area per warp), and a persistent grid of as many blocks as can be
 // resident (optionally capped per SM), but no more than there are items.
+// Resident blocks per SM of a class kernel for a launch shape: the same for every
+// context on a device, so asked once (the query costs tens of microseconds).
+static cudaError_t occupancy(int device, int ci, int part, int wpb, size_t smem, int* bps) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int, size_t>, int> cache;
+    const auto key = std::make_tuple(device, ci, part, wpb, smem);
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) { *bps = it->second; return cudaSuccess; }
+    }
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, g_classes[ci].kernel(part == 1), 32 * wpb, smem);
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> g(mu);
+        cache[key] = *bps;
+    }
+    return e;
+}
+
 static int class_launch_shape(qk_ctx* c, int ci) {
     const ClassEntry& ce = g_classes[ci];
     ClassWork& W = c->work[ci];
@@ -1333,12 +1360,12 @@ static int class_launch_shape(qk_ctx* c, int ci) {
     if (smem > 48 * 1024)
         QK_CUDA_TRY(cudaFuncSetAttribute(ce.kernel(false), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ce.smem));
     for (int part = 0; part < 2; ++part) {
-        const long long n = part == 0 ? W.n64 : (long long)W.items.size() - W.n64;
+        const long long n = part == 0 ? W.n64 : (long long)W.n_items - W.n64;
         int& grid = part == 0 ? W.grid : W.grid32;
         grid = 0;
         if (n <= 0) continue;
         int bps = 0;
-        QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ce.kernel(part == 1), 32 * wpb, smem));
+        QK_CUDA_TRY(occupancy(c->device, ci, part, wpb, smem, &bps));
         if (bps < 1) return fail(QK_ERR_CUDA, "class kernel cannot be resident");
         if (c->cls_bpsm[ci] > 0) bps = std::min(bps, c->cls_bpsm[ci]);
         grid = (int)std::max<long long>(1, std::min<long long>((long long)bps * c->num_sms, (n + wpb - 1) / wpb));
@@ -1348,10 +1375,14 @@ static int class_launch_shape(qk_ctx* c, int ci) {
     return QK_OK;
 }
 
+static int finish_work(qk_ctx* c);
+
+// Work items of every class built on the host (the reference implementation of
+// the lists; the device builder, build_work_device, gives the same lists and is
+// the default except for sharded contexts).
 static int build_work(qk_ctx* c) {
     PairTable& T = c->pairs;
     const double cut = c->integralCutoff;
-    c->launches = 0;
     for (int ci = 0; ci < kNumClasses; ++ci) {
         const ClassEntry& ce = g_classes[ci];
         ClassWork& W = c->work[ci];
@@ -1427,17 +1458,35 @@ static int build_work(qk_ctx* c) {
         for (const Tmp& t : tmp) W.n64 += t.it.w == 0;
         W.items.resize(tmp.size());
         for (size_t i = 0; i < tmp.size(); ++i) W.items[i] = tmp[i].it;
-        QK_CUDA_TRY(W.d_items.upload(W.items, c->stream));
-        if (!W.items.empty()) {
+        W.n_items = (int)W.items.size();
+    }
+    // one device buffer for every class's items, class after class
+    std::vector<int4> all;
+    std::vector<size_t> first(kNumClasses);
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        first[ci] = all.size();
+        all.insert(all.end(), c->work[ci].items.begin(), c->work[ci].items.end());
+    }
+    QK_CUDA_TRY(c->d_items.upload(all, c->stream));
+    for (int ci = 0; ci < kNumClasses; ++ci) c->work[ci].d_items = c->d_items.p + first[ci];
+    return finish_work(c);
+}
+
+// Launch shapes, launch count and launch order of the work lists just built.
+static int finish_work(qk_ctx* c) {
+    c->launches = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        ClassWork& W = c->work[ci];
+        if (W.n_items > 0) {
             int st = class_launch_shape(c, ci);
             if (st) return st;
-            c->launches += (W.n64 > 0) + (W.n64 < (int)W.items.size());
+            c->launches += (W.n64 > 0) + (W.n64 < W.n_items);
         }
     }
     c->launches += 1;  // finalize
     c->launch_order.clear();
     for (int ci = 0; ci < kNumClasses; ++ci)
-        if (!c->work[ci].items.empty()) c->launch_order.push_back(ci);
+        if (c->work[ci].n_items > 0) c->launch_order.push_back(ci);
     std::stable_sort(c->launch_order.begin(), c->launch_order.end(), [&](int x, int y) {
         if (g_classes[x].coop != g_classes[y].coop) return g_classes[x].coop;
         const double wx = c->work[x].nprimq * g_classes[x].prim_flops + c->work[x].nquart * g_classes[x].quartet_flops;
@@ -1454,6 +1503,216 @@ static int build_work(qk_ctx* c) {
     return QK_OK;
 }
 
+// ------------------------------------------------------------------ work lists on the device
+// The same lists as build_work, built by the GPU: a segment is one (bra bucket,
+// ket bucket) pair of a class, and one thread per (segment, bra pair) finds its
+// ket prefix by binary search (wl_count_kernel); exclusive scans of the FP64 and
+// FP32 item counts give every thread its place (wl_emit_kernel).  The segments of
+// a class are ordered by cost on the host exactly as build_work's stable sort
+// orders the items, so the lists are identical item for item.
+struct WlSeg {
+    int bra0, bra1;        // bra pairs [bra0, bra1)
+    int ket0, ket1;        // ket bucket [ket0, ket1), Y descending
+    int ci;                // class
+    int chunk;             // kets per item: 32 (per-lane classes) or 1 (cooperative)
+    int tri;               // bra and ket bucket are the same: kets Q <= P only
+    int fp32_ok;           // the mixed form may put this segment's small-bound kets in FP32 items
+    long long ket_npp;     // primitive pairs of one ket pair
+    int t0;                // first thread of the segment
+    int pad;
+};
+
+__device__ __forceinline__ int wl_find_seg(const WlSeg* __restrict__ segs, int nseg, int t) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].t0 <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void wl_count_kernel(const WlSeg* __restrict__ segs, int nseg, int nthreads, const double* __restrict__ Y,
+                                const int* __restrict__ npp, double cut, double fp32_bound, int* __restrict__ nk_out,
+                                int* __restrict__ n64_out, int* __restrict__ c64, int* __restrict__ c32,
+                                unsigned long long* __restrict__ stats) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nthreads) return;
+    const WlSeg sg = segs[wl_find_seg(segs, nseg, t)];
+    const int P = sg.bra0 + (t - sg.t0);
+    const double yp = Y[P];
+    int lo = sg.ket0, hi = sg.ket1;
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (yp * Y[mid] > cut) lo = mid + 1; else hi = mid;
+    }
+    int nk = lo - sg.ket0;
+    if (sg.tri) nk = min(nk, P - sg.bra0 + 1);
+    int n64 = nk;
+    if (nk > 0 && fp32_bound > 0.0 && sg.fp32_ok) {
+        int a = 0, z = nk;
+        while (a < z) {
+            const int mid = (a + z) / 2;
+            if (yp * Y[sg.ket0 + mid] >= fp32_bound) a = mid + 1; else z = mid;
+        }
+        n64 = a;
+    }
+    if (nk < 0) nk = 0;
+    nk_out[t] = nk;
+    n64_out[t] = n64;
+    c64[t] = nk > 0 ? (n64 + sg.chunk - 1) / sg.chunk : 0;
+    c32[t] = nk > 0 ? (nk - n64 + sg.chunk - 1) / sg.chunk : 0;
+    if (nk > 0) {
+        atomicAdd(stats + 3 * sg.ci, (unsigned long long)nk);
+        atomicAdd(stats + 3 * sg.ci + 1, (unsigned long long)npp[P] * (unsigned long long)sg.ket_npp * nk);
+        atomicAdd(stats + 3 * sg.ci + 2, (unsigned long long)(nk - n64));
+    }
+}
+
+// per class: FP64 and FP32 item totals from the scans (threads [t0, t1) of the class)
+__global__ void wl_totals_kernel(const int* __restrict__ ct0, const int* __restrict__ ct1, const int* __restrict__ c64,
+                                 const int* __restrict__ off64, const int* __restrict__ c32,
+                                 const int* __restrict__ off32, int ncls, int* __restrict__ tot) {
+    const int ci = threadIdx.x;
+    if (ci >= ncls) return;
+    const int a = ct0[ci], b = ct1[ci];
+    tot[2 * ci] = b > a ? off64[b - 1] + c64[b - 1] - off64[a] : 0;
+    tot[2 * ci + 1] = b > a ? off32[b - 1] + c32[b - 1] - off32[a] : 0;
+}
+
+// cls: per class [first thread, item base, FP64 items]
+__global__ void wl_emit_kernel(const WlSeg* __restrict__ segs, int nseg, int nthreads, const int* __restrict__ nk_in,
+                               const int* __restrict__ n64_in, const int* __restrict__ off64,
+                               const int* __restrict__ off32, const int* __restrict__ cls, int4* __restrict__ items) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nthreads) return;
+    const int nk = nk_in[t];
+    if (nk <= 0) return;
+    const WlSeg sg = segs[wl_find_seg(segs, nseg, t)];
+    const int P = sg.bra0 + (t - sg.t0);
+    const int n64 = n64_in[t];
+    const int first = cls[3 * sg.ci], base = cls[3 * sg.ci + 1], n64c = cls[3 * sg.ci + 2];
+    int4* o = items + base + (off64[t] - off64[first]);
+    for (int k = 0; k < n64; k += sg.chunk) *o++ = make_int4(P, sg.ket0 + k, min(sg.chunk, n64 - k), 0);
+    o = items + base + n64c + (off32[t] - off32[first]);
+    for (int k = n64; k < nk; k += sg.chunk) *o++ = make_int4(P, sg.ket0 + k, min(sg.chunk, nk - k), 1);
+}
+
+static size_t wl_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// build_work on the GPU (pair tables already uploaded on the context stream); two
+// small host synchronisations: the class totals, and the end of prepare.
+static int build_work_device(qk_ctx* c) {
+    PairTable& T = c->pairs;
+    cudaStream_t s = c->stream;
+    // segments, class by class, each class's in build_work's item order
+    std::vector<WlSeg> segs;
+    std::vector<int> ct0(kNumClasses), ct1(kNumClasses);
+    int nthreads = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        const ClassEntry& ce = g_classes[ci];
+        const bool same = (ce.La == ce.Lc && ce.Lb == ce.Ld);
+        struct Cand { WlSeg sg; long long cost; };
+        std::vector<Cand> cand;
+        for (int bb = 0; bb < (int)T.buckets.size(); ++bb) {
+            const Bucket& B = T.buckets[bb];
+            if (B.La != ce.La || B.Lb != ce.Lb) continue;
+            for (int kb = 0; kb < (int)T.buckets.size(); ++kb) {
+                const Bucket& K = T.buckets[kb];
+                if (K.La != ce.Lc || K.Lb != ce.Ld) continue;
+                if (same && kb > bb) continue;
+                WlSeg sg{};
+                sg.bra0 = B.begin; sg.bra1 = B.end; sg.ket0 = K.begin; sg.ket1 = K.end;
+                sg.ci = ci; sg.chunk = ce.coop ? 1 : 32; sg.tri = (same && kb == bb) ? 1 : 0;
+                sg.fp32_ok = ce.coop ? 0 : 1;
+                sg.ket_npp = (long long)K.npa * K.npb;
+                cand.push_back({sg, (long long)B.npa * B.npb * K.npa * K.npb});
+            }
+        }
+        std::stable_sort(cand.begin(), cand.end(), [](const Cand& x, const Cand& y) { return x.cost > y.cost; });
+        ct0[ci] = nthreads;
+        for (auto& cd : cand) {
+            cd.sg.t0 = nthreads;
+            nthreads += cd.sg.bra1 - cd.sg.bra0;
+            segs.push_back(cd.sg);
+        }
+        ct1[ci] = nthreads;
+    }
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        ClassWork& W = c->work[ci];
+        W.items.clear();
+        W.nquart = W.nprimq = W.nquart32 = 0;
+        W.n64 = W.n_items = 0;
+        W.d_items = nullptr;
+    }
+    if (nthreads == 0) return finish_work(c);
+    const int nseg = (int)segs.size();
+    // scratch layout
+    size_t cub_bytes = 0;
+    QK_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (int*)nullptr, (int*)nullptr, nthreads, s));
+    const size_t nt = (size_t)nthreads;
+    size_t off = 0;
+    const size_t o_seg = off; off = wl_align(off + sizeof(WlSeg) * nseg);
+    const size_t o_nk = off; off = wl_align(off + 4 * nt);
+    const size_t o_n64 = off; off = wl_align(off + 4 * nt);
+    const size_t o_c64 = off; off = wl_align(off + 4 * nt);
+    const size_t o_c32 = off; off = wl_align(off + 4 * nt);
+    const size_t o_off64 = off; off = wl_align(off + 4 * nt);
+    const size_t o_off32 = off; off = wl_align(off + 4 * nt);
+    const size_t o_stats = off; off = wl_align(off + 8 * 3 * kNumClasses);
+    const size_t o_ct = off; off = wl_align(off + 4 * 2 * kNumClasses);
+    const size_t o_tot = off; off = wl_align(off + 4 * 2 * kNumClasses);
+    const size_t o_cls = off; off = wl_align(off + 4 * 3 * kNumClasses);
+    const size_t o_cub = off; off = wl_align(off + cub_bytes);
+    QK_CUDA_TRY(c->d_wl.reserve(off));
+    char* w = c->d_wl.p;
+    WlSeg* d_seg = (WlSeg*)(w + o_seg);
+    int *d_nk = (int*)(w + o_nk), *d_n64 = (int*)(w + o_n64), *d_c64 = (int*)(w + o_c64), *d_c32 = (int*)(w + o_c32);
+    int *d_off64 = (int*)(w + o_off64), *d_off32 = (int*)(w + o_off32);
+    unsigned long long* d_stats = (unsigned long long*)(w + o_stats);
+    int *d_ct = (int*)(w + o_ct), *d_tot = (int*)(w + o_tot), *d_cls = (int*)(w + o_cls);
+    std::vector<int> ct(2 * kNumClasses);
+    for (int ci = 0; ci < kNumClasses; ++ci) { ct[ci] = ct0[ci]; ct[kNumClasses + ci] = ct1[ci]; }
+    QK_CUDA_TRY(cudaMemcpyAsync(d_seg, segs.data(), sizeof(WlSeg) * nseg, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(d_ct, ct.data(), sizeof(int) * 2 * kNumClasses, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaMemsetAsync(d_stats, 0, 8 * 3 * kNumClasses, s));
+    const int nb = (nthreads + 255) / 256;
+    wl_count_kernel<<<nb, 256, 0, s>>>(d_seg, nseg, nthreads, T.d_Y.p, T.d_npp.p, c->integralCutoff, c->fp32_bound,
+                                       d_nk, d_n64, d_c64, d_c32, d_stats);
+    QK_CUDA_TRY(cudaGetLastError());
+    size_t tb = cub_bytes;
+    QK_CUDA_TRY(cub::DeviceScan::ExclusiveSum(w + o_cub, tb, d_c64, d_off64, nthreads, s));
+    tb = cub_bytes;
+    QK_CUDA_TRY(cub::DeviceScan::ExclusiveSum(w + o_cub, tb, d_c32, d_off32, nthreads, s));
+    wl_totals_kernel<<<1, 64, 0, s>>>(d_ct, d_ct + kNumClasses, d_c64, d_off64, d_c32, d_off32, kNumClasses, d_tot);
+    QK_CUDA_TRY(cudaGetLastError());
+    std::vector<int> tot(2 * kNumClasses);
+    std::vector<unsigned long long> st(3 * kNumClasses);
+    QK_CUDA_TRY(cudaMemcpyAsync(tot.data(), d_tot, sizeof(int) * 2 * kNumClasses, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(st.data(), d_stats, 8 * 3 * kNumClasses, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int> cls(3 * kNumClasses);
+    long long total = 0;
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+        ClassWork& W = c->work[ci];
+        W.n64 = tot[2 * ci];
+        W.n_items = tot[2 * ci] + tot[2 * ci + 1];
+        W.nquart = (long long)st[3 * ci];
+        W.nprimq = (long long)st[3 * ci + 1];
+        W.nquart32 = (long long)st[3 * ci + 2];
+        cls[3 * ci] = ct0[ci];
+        cls[3 * ci + 1] = (int)total;
+        cls[3 * ci + 2] = W.n64;
+        total += W.n_items;
+    }
+    if (total > INT_MAX) return fail(QK_ERR_UNSUPPORTED, "more than 2^31 work items");
+    QK_CUDA_TRY(c->d_items.reserve((size_t)std::max<long long>(total, 1)));
+    QK_CUDA_TRY(cudaMemcpyAsync(d_cls, cls.data(), sizeof(int) * 3 * kNumClasses, cudaMemcpyHostToDevice, s));
+    wl_emit_kernel<<<nb, 256, 0, s>>>(d_seg, nseg, nthreads, d_nk, d_n64, d_off64, d_off32, d_cls, c->d_items.p);
+    QK_CUDA_TRY(cudaGetLastError());
+    for (int ci = 0; ci < kNumClasses; ++ci) c->work[ci].d_items = c->d_items.p + cls[3 * ci + 1];
+    return finish_work(c);
+}
+
 static int ensure_pairs(qk_ctx* c) {
     if (!c->have_basis) return fail(QK_ERR_NOT_READY, "basis not uploaded");
     if (!c->have_schwarz) return fail(QK_ERR_NOT_READY, "Schwarz bounds not set");
@@ -1465,7 +1724,8 @@ static int ensure_pairs(qk_ctx* c) {
     build_pairs(c, true);
     int st = upload_pairs(c);
     if (st) return st;
-    st = build_work(c);
+    // the device builder, except for sharded contexts (the host one deals items to shards)
+    st = (c->worklist_on_device && c->shard_count == 1) ? build_work_device(c) : build_work(c);
     if (st) return st;
     // tables were uploaded on the context stream; builds may run on another stream
     QK_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1479,11 +1739,11 @@ static int ensure_pairs(qk_ctx* c) {
 // part with its own counter (counters[ci] and counters[kNumClasses + ci]).
 static void launch_class(const ClassEntry& ce, const ClassWork& W, cudaStream_t s, const DevData& d, int* counters,
                          int ci) {
-    const int n = (int)W.items.size();
+    const int n = W.n_items;
     if (W.n64 > 0)
-        ce.fn(false, dim3(W.grid), dim3(W.block), W.smem, s, d, W.d_items.p, W.n64, counters + ci);
+        ce.fn(false, dim3(W.grid), dim3(W.block), W.smem, s, d, W.d_items, W.n64, counters + ci);
     if (n > W.n64)
-        ce.fn(true, dim3(W.grid32), dim3(W.block), W.smem, s, d, W.d_items.p + W.n64, n - W.n64,
+        ce.fn(true, dim3(W.grid32), dim3(W.block), W.smem, s, d, W.d_items + W.n64, n - W.n64,
               counters + kNumClasses + ci);
 }
 
@@ -1764,7 +2024,12 @@ qk_ctx* qk_create(int device, int* status) {
     c->device = device;
     c->maxprim = g_maxprim_default;
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // the context's own stream (tables, work lists, Schwarz bounds) at the highest
+    // priority: a set-up that runs beside other contexts' long Fock builds gets the
+    // SMs as soon as one of their kernels ends
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess) {
         delete c;
         if (status) *status = fail(QK_ERR_CUDA, "stream creation failed");
         return nullptr;
@@ -2174,7 +2439,7 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
     constexpr int kSlots = 2 * kNumClasses;
     auto part_range = [&](const ClassWork& W, int slot, int* first, int* count) {
         *first = slot < kNumClasses ? 0 : W.n64;
-        *count = slot < kNumClasses ? W.n64 : (int)W.items.size() - W.n64;
+        *count = slot < kNumClasses ? W.n64 : W.n_items - W.n64;
     };
     int seg_count[kSlots], seg_off[kSlots], total_items[kSlots];
     int nseg_all = 0;
@@ -2241,7 +2506,7 @@ int qk_batch_fock2e(qk_batch* b, int n, qk_ctx* const* ctxs, const double* const
             int f, cnt;
             part_range(W, slot, &f, &cnt);
             if (cnt <= 0) continue;
-            sg[ns++] = BatchSeg{W.d_items.p + f, at, m};
+            sg[ns++] = BatchSeg{W.d_items + f, at, m};
             at += cnt;
         }
     }
@@ -2292,7 +2557,7 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     std::lock_guard<std::mutex> g(c->mu);
     const PairTable& T = c->pairs;
     unsigned long long it = 0;
-    for (int ci = 0; ci < kNumClasses; ++ci) it += c->work[ci].d_items.bytes();
+    it += c->d_items.bytes() + c->d_wl.bytes();
     unsigned long long t = it;
     for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
                      T.d_Y.bytes(), T.d_zo.bytes(), T.d_kc.bytes(), T.d_pxy.bytes(), T.d_pzax.bytes(),
@@ -2326,7 +2591,7 @@ int qk_set_class_launch(qk_ctx* c, int ci, int warps_per_block, int blocks_per_s
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
     c->cls_wpb[ci] = warps_per_block;
     c->cls_bpsm[ci] = blocks_per_sm;
-    if (!c->work[ci].items.empty()) return class_launch_shape(c, ci);
+    if (c->work[ci].n_items > 0) return class_launch_shape(c, ci);
     return QK_OK;
 }
 
@@ -2340,7 +2605,17 @@ int qk_class_launch(qk_ctx* c, int ci, int* warps_per_block, int* max_warps, int
                                        : (c->cls_wpb[ci] > 0 ? c->cls_wpb[ci] : (ce.coop ? ce.coop_warps : kWarpsPerBlock));
     if (max_warps) *max_warps = ce.coop ? ce.coop_warps : kMaxLaneWarps;
     if (blocks_per_sm) *blocks_per_sm = c->cls_bpsm[ci];
-    if (grid) *grid = W.items.empty() ? 0 : W.grid;
+    if (grid) *grid = W.n_items == 0 ? 0 : W.grid;
+    return QK_OK;
+}
+
+int qk_set_worklist_builder(qk_ctx* c, int on_device) {
+    if (!c || (on_device != 0 && on_device != 1)) return fail(QK_ERR_INVALID_ARG, "qk_set_worklist_builder: 0 or 1");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (c->worklist_on_device != (on_device == 1)) {
+        c->worklist_on_device = on_device == 1;
+        c->pairs_dirty = true;
+    }
     return QK_OK;
 }
 

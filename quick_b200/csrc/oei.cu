@@ -375,7 +375,12 @@ static cudaStream_t oei_stream(int device) {
     static cudaStream_t streams[64] = {};
     std::lock_guard<std::mutex> g(mu);
     if (device < 0 || device >= 64) return nullptr;
-    if (!streams[device]) cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking);
+    if (!streams[device]) {
+        // highest priority, as the contexts' set-up streams (see qk_create)
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        cudaStreamCreateWithPriority(&streams[device], cudaStreamNonBlocking, hi);
+    }
     return streams[device];
 }
 

@@ -202,6 +202,10 @@ class Get2e:
         import torch.distributed as dist
         self.set_shard(dist.get_rank(group), dist.get_world_size(group))
 
+    def set_worklist_builder(self, on_device: bool):
+        """Build the work lists on the GPU (default) or on the host (same lists)."""
+        check(lib().qk_set_worklist_builder(self.h, int(bool(on_device))), "qk_set_worklist_builder")
+
     def set_streams(self, nstreams: int):
         """Class kernels over ``nstreams`` concurrent streams (0: one after another)."""
         check(lib().qk_set_streams(self.h, int(nstreams)), "qk_set_streams")

@@ -289,7 +289,8 @@ class Server:
         st = getattr(self._tls, "stream", None)
         if st is None:
             self.torch.cuda.set_device(self.device)
-            st = self._tls.stream = self.torch.cuda.Stream(self.device, priority=0)
+            # high priority: the set-up's kernels get SMs at the batch kernels' boundaries
+            st = self._tls.stream = self.torch.cuda.Stream(self.device, priority=-1)
         return st
 
     def _setup(self, req, eng, D0):
@@ -569,10 +570,11 @@ def _max_dE(results, ref_E):
 
 
 def run_stream(n_requests: int, rate: float, fp32_bound: float = 0.0, seed: int = 20261203,
-               memory_budget: int = None, denserms: float = 1e-6, device: int = 0, **stream_kw):
+               memory_budget: int = None, denserms: float = 1e-6, device: int = 0, workers: int = 4, **stream_kw):
     """Serve one seeded stream; returns (summary dict, results)."""
     reqs = request_stream(n_requests, rate, seed=seed, **stream_kw)
-    srv = Server(device=device, memory_budget=memory_budget, fp32_bound=fp32_bound, denserms=denserms)
+    srv = Server(device=device, memory_budget=memory_budget, fp32_bound=fp32_bound, denserms=denserms,
+                 workers=workers)
     try:
         res = srv.serve(reqs, realtime=True)
         s = summarize(res, srv.wall)
@@ -604,6 +606,7 @@ def main(argv=None):
     ap.add_argument("--compare", action="store_true",
                     help="serve each stream in plain FP64 and in the mixed form; report |dE| per request")
     ap.add_argument("--budget-gb", type=float, default=None)
+    ap.add_argument("--workers", type=int, default=4, help="set-up threads")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--out", default=None)
     ap.add_argument("--warmup", type=int, default=64,
@@ -614,7 +617,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     budget = int(a.budget_gb * (1 << 30)) if a.budget_gb else None
     if a.warmup > 0:
-        w = Server(memory_budget=budget)
+        w = Server(memory_budget=budget, workers=a.workers)
         w.serve(request_stream(a.warmup, 1000.0, seed=a.seed + 1), realtime=False)
         w.close()
     report = []
@@ -625,9 +628,9 @@ def main(argv=None):
         report.append({"sequential_fp64": seq})
     for rate in a.rate:
         if a.compare:
-            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget)
+            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget, workers=a.workers)
             bound = a.fp32_bound if a.fp32_bound > 0 else 1e-5
-            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget)
+            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget, workers=a.workers)
             e64 = {r.rid: r.E for r in r64}
             dE = [abs(r.E - e64[r.rid]) for r in r32 if r.rid in e64]
             s32["max_abs_dE_vs_fp64"] = float(max(dE)) if dE else None
@@ -640,7 +643,7 @@ def main(argv=None):
                 line["mixed_vs_sequential_fp64"] = s32["solves_per_s"] / seq["solves_per_s"]
                 line["fp64_vs_sequential_fp64"] = s64["solves_per_s"] / seq["solves_per_s"]
         else:
-            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget)
+            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget, workers=a.workers)
             if seq:
                 line["vs_sequential_fp64"] = line["solves_per_s"] / seq["solves_per_s"]
         print(json.dumps(line), flush=True)
