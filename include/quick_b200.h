@@ -81,6 +81,13 @@ void gpu_upload_cutoff_(double *cutMatrix, double *integralCutoff, double *primL
 /* replaces gpu_get_cshell_eri_ (src/gpu/gpu_get2e_getxc_drivers.h:27, declared at
  * src/gpu/cuda/gpu.h:65): o(nbasis,nbasis) += G(dense), G = J - K/2 */
 void gpu_get_cshell_eri_(bool *deltaO, double *o);
+/* replaces gpu_upload_calculated_beta_ (src/gpu/cuda/gpu.cu, declared at src/gpu/cuda/gpu.h:33):
+ * the beta density `denseb` (nbasis^2) of an open-shell (UHF) build */
+void gpu_upload_calculated_beta_(double *ob, double *denseb);
+/* replaces gpu_get_oshell_eri_ (src/gpu/gpu_get2e_getxc_drivers.h:24-25 under OSHELL):
+ * o += G_alpha, ob += G_beta from the densities of gpu_upload_calculated_ (alpha) and
+ * gpu_upload_calculated_beta_ (beta) and the open-shell density screen of gpu_upload_cutoff_ */
+void gpu_get_oshell_eri_(bool *deltaO, double *o, double *ob);
 /* replaces gpu_delete_ (src/gpu/cuda/gpu.cu:514) */
 void gpu_delete_(int *ierr);
 
@@ -157,6 +164,19 @@ int qk_fock2e_host(qk_ctx *ctx, const double *D, const double *cutmat, double *o
 /* Density screen on the device: cutmat_dev(nshell,nshell) = max |D| per shell pair
  * (stream: a cudaStream_t, NULL = the CUDA default stream). */
 int qk_density_cutoff_device(qk_ctx *ctx, const double *D_dev, double *cutmat_dev, void *stream);
+
+/* Open-shell (UHF) Fock build (replaces get_oshell_eri, src/modules/include/eri.fh under
+ * OSHELL, and its GPU form src/gpu/gpu_get2e_subs.h:638-660): oa_dev += G_alpha,
+ * ob_dev += G_beta with G_alpha = J[Da + Db] - K[Da] and G_beta = J[Da + Db] - K[Db]
+ * (HF exchange).  cutmat_dev: QUICK's open-shell density screen (per shell pair the
+ * largest of |Da + Db|, |Da|, |Db|; oshell_density_cutoff, src/modules/include/cutoff.fh)
+ * or NULL to derive it on the device.  Computed as a closed-shell build of Da + Db and an
+ * exchange-only build of Da - Db on the same screened quartets; bit-reproducible.
+ * Enqueued on `stream`, no synchronisation; the _host form copies and synchronises. */
+int qk_fock2e_uhf_device(qk_ctx *ctx, const double *Da_dev, const double *Db_dev, const double *cutmat_dev,
+                         double *oa_dev, double *ob_dev, void *stream);
+int qk_fock2e_uhf_host(qk_ctx *ctx, const double *Da, const double *Db, const double *cutmat, double *oa,
+                       double *ob);
 
 /* Allocation-free Fock build (no counterpart in the reference).  Same arguments and
  * result as qk_fock2e_device, for callers that must not allocate device memory at the

@@ -339,7 +339,7 @@ void hrr_expand(const int a[3], const int b[3], const double AB[3], double coef,
 // the index-equality branches of src/modules/include/eri.fh:649-1050.
 struct Ctx {
     const Basis* B;
-    const double* dense;      // nbasis^2 col-major
+    const double* dense;      // nbasis^2 col-major: the density of the J terms
     const double* cutmatrix;  // nshell^2
     const double* cutprim;    // jbasis^2
     double integralCutoff, primLimit;
@@ -349,6 +349,9 @@ struct Ctx {
     // (src/gpu/gpu_get2e_subs.h:389).  gpu_screens reproduces both, to compare
     // with that implementation; off, this is the CPU get2e.
     bool gpu_screens = false;
+    // density of the K terms when it differs from `dense` (an open-shell matrix: 2 Da
+    // or 2 Db against J's Da + Db); null = the same
+    const double* dense_k = nullptr;
 };
 
 inline double& O(double* G, int n, int r, int c) { return G[(size_t)(r - 1) + (size_t)n * (c - 1)]; }
@@ -469,8 +472,15 @@ void cshell_quartet(const Ctx& C, Work& W, int II, int JJ, int KK, int LL, doubl
                             for (auto& r : hr) y += l.second * r.second * W.store[l.first * NCART_TOT + r.first];
                         return y * B.cons[iii - 1] * B.cons[jjj - 1] * B.cons[kkk - 1] * B.cons[lll - 1];
                     };
-                    const double* D = C.dense;
+                    // J terms read DJ, K terms read DK: the closed-shell build has DJ = DK = D;
+                    // the open-shell (OSHELL) branches of eri.fh are the same updates with
+                    // DJ = Da + Db and, for the alpha (beta) matrix, DK = 2 Da (2 Db), the
+                    // K coefficients of the closed shell halved against the total density.
+                    const double* DJ = C.dense;
+                    const double* DK = C.dense_k ? C.dense_k : C.dense;
                     const double hx = 1.0;  // x_hybrid_coeff for HF
+                    auto J = [&](int r, int cc) { return Dn(DJ, n, r, cc); };
+                    auto K = [&](int r, int cc) { return Dn(DK, n, r, cc); };
                     if (II < JJ && II < KK && KK < LL) {
                         for (int III = III1; III <= III2; ++III)
                             for (int JJJ = JJJ1; JJJ <= JJJ2; ++JJJ)
@@ -478,17 +488,14 @@ void cshell_quartet(const Ctx& C, Work& W, int II, int JJ, int KK, int LL, doubl
                                     for (int LLL = LLL1; LLL <= LLL2; ++LLL) {
                                         double Y = hrrwhole(III, JJJ, KKK, LLL);
                                         if (C.gpu_screens && !(std::fabs(Y) > C.integralCutoff)) continue;
-                                        double DKI = Dn(D, n, KKK, III), DKJ = Dn(D, n, KKK, JJJ);
-                                        double DLJ = Dn(D, n, LLL, JJJ), DLI = Dn(D, n, LLL, III);
-                                        double DLK = Dn(D, n, LLL, KKK), DJI = Dn(D, n, JJJ, III);
-                                        O(Gm, n, JJJ, III) += 2.0 * DLK * Y;
-                                        O(Gm, n, LLL, KKK) += 2.0 * DJI * Y;
-                                        O(Gm, n, KKK, III) -= hx * 0.5 * DLJ * Y;
-                                        O(Gm, n, LLL, III) -= hx * 0.5 * DKJ * Y;
-                                        O(Gm, n, JJJ, KKK) -= hx * 0.5 * DLI * Y;
-                                        O(Gm, n, JJJ, LLL) -= hx * 0.5 * DKI * Y;
-                                        O(Gm, n, KKK, JJJ) -= hx * 0.5 * DLI * Y;
-                                        O(Gm, n, LLL, JJJ) -= hx * 0.5 * DKI * Y;
+                                        O(Gm, n, JJJ, III) += 2.0 * J(LLL, KKK) * Y;
+                                        O(Gm, n, LLL, KKK) += 2.0 * J(JJJ, III) * Y;
+                                        O(Gm, n, KKK, III) -= hx * 0.5 * K(LLL, JJJ) * Y;
+                                        O(Gm, n, LLL, III) -= hx * 0.5 * K(KKK, JJJ) * Y;
+                                        O(Gm, n, JJJ, KKK) -= hx * 0.5 * K(LLL, III) * Y;
+                                        O(Gm, n, JJJ, LLL) -= hx * 0.5 * K(KKK, III) * Y;
+                                        O(Gm, n, KKK, JJJ) -= hx * 0.5 * K(LLL, III) * Y;
+                                        O(Gm, n, LLL, JJJ) -= hx * 0.5 * K(KKK, III) * Y;
                                     }
                     } else {
                         for (int III = III1; III <= III2; ++III)
@@ -499,64 +506,50 @@ void cshell_quartet(const Ctx& C, Work& W, int II, int JJ, int KK, int LL, doubl
                                             double Y = hrrwhole(III, JJJ, KKK, LLL);
                                             if (C.gpu_screens && !(std::fabs(Y) > C.integralCutoff)) continue;
                                             if (III < JJJ && KKK < LLL) {
-                                                double DKI = Dn(D, n, KKK, III), DKJ = Dn(D, n, KKK, JJJ);
-                                                double DLJ = Dn(D, n, LLL, JJJ), DLI = Dn(D, n, LLL, III);
-                                                double DLK = Dn(D, n, LLL, KKK), DJI = Dn(D, n, JJJ, III);
-                                                O(Gm, n, JJJ, III) += 2.0 * DLK * Y;
-                                                O(Gm, n, LLL, KKK) += 2.0 * DJI * Y;
-                                                O(Gm, n, KKK, III) -= hx * 0.5 * DLJ * Y;
-                                                O(Gm, n, LLL, III) -= hx * 0.5 * DKJ * Y;
-                                                O(Gm, n, JJJ, KKK) -= hx * 0.5 * DLI * Y;
-                                                O(Gm, n, JJJ, LLL) -= hx * 0.5 * DKI * Y;
-                                                O(Gm, n, KKK, JJJ) -= hx * 0.5 * DLI * Y;
-                                                O(Gm, n, LLL, JJJ) -= hx * 0.5 * DKI * Y;
+                                                O(Gm, n, JJJ, III) += 2.0 * J(LLL, KKK) * Y;
+                                                O(Gm, n, LLL, KKK) += 2.0 * J(JJJ, III) * Y;
+                                                O(Gm, n, KKK, III) -= hx * 0.5 * K(LLL, JJJ) * Y;
+                                                O(Gm, n, LLL, III) -= hx * 0.5 * K(KKK, JJJ) * Y;
+                                                O(Gm, n, JJJ, KKK) -= hx * 0.5 * K(LLL, III) * Y;
+                                                O(Gm, n, JJJ, LLL) -= hx * 0.5 * K(KKK, III) * Y;
+                                                O(Gm, n, KKK, JJJ) -= hx * 0.5 * K(LLL, III) * Y;
+                                                O(Gm, n, LLL, JJJ) -= hx * 0.5 * K(KKK, III) * Y;
                                             } else if (III == JJJ && KKK == LLL) {
-                                                double DJI = Dn(D, n, KKK, III), DJJ = Dn(D, n, KKK, KKK), DII = Dn(D, n, III, III);
-                                                O(Gm, n, III, III) += DJJ * Y;
-                                                O(Gm, n, KKK, KKK) += DII * Y;
-                                                O(Gm, n, KKK, III) -= hx * 0.5 * DJI * Y;
+                                                O(Gm, n, III, III) += J(KKK, KKK) * Y;
+                                                O(Gm, n, KKK, KKK) += J(III, III) * Y;
+                                                O(Gm, n, KKK, III) -= hx * 0.5 * K(KKK, III) * Y;
                                             } else if (JJJ == KKK && JJJ == LLL) {
-                                                double DJI = Dn(D, n, JJJ, III), DJJ = Dn(D, n, JJJ, JJJ);
-                                                O(Gm, n, JJJ, III) += DJJ * Y - hx * 0.5 * DJJ * Y;
-                                                O(Gm, n, JJJ, JJJ) += 2.0 * DJI * Y - hx * DJI * Y;
+                                                O(Gm, n, JJJ, III) += J(JJJ, JJJ) * Y - hx * 0.5 * K(JJJ, JJJ) * Y;
+                                                O(Gm, n, JJJ, JJJ) += 2.0 * J(JJJ, III) * Y - hx * K(JJJ, III) * Y;
                                             } else if (KKK == LLL && III < JJJ && JJJ != KKK) {
-                                                double DKI = Dn(D, n, KKK, III), DKJ = Dn(D, n, KKK, JJJ);
-                                                double DKK = Dn(D, n, KKK, KKK), DJI = Dn(D, n, JJJ, III);
-                                                O(Gm, n, JJJ, III) += DKK * Y;
-                                                O(Gm, n, KKK, KKK) += 2.0 * DJI * Y;
-                                                O(Gm, n, KKK, III) -= hx * 0.5 * DKJ * Y;
-                                                O(Gm, n, KKK, JJJ) -= hx * 0.5 * DKI * Y;
-                                                O(Gm, n, JJJ, KKK) -= hx * 0.5 * DKI * Y;
+                                                O(Gm, n, JJJ, III) += J(KKK, KKK) * Y;
+                                                O(Gm, n, KKK, KKK) += 2.0 * J(JJJ, III) * Y;
+                                                O(Gm, n, KKK, III) -= hx * 0.5 * K(KKK, JJJ) * Y;
+                                                O(Gm, n, KKK, JJJ) -= hx * 0.5 * K(KKK, III) * Y;
+                                                O(Gm, n, JJJ, KKK) -= hx * 0.5 * K(KKK, III) * Y;
                                             } else if (III == JJJ && KKK < LLL) {
-                                                double DII = Dn(D, n, III, III), DJI = Dn(D, n, KKK, III);
-                                                double DKI = Dn(D, n, LLL, III), DKJ = Dn(D, n, LLL, KKK);
-                                                O(Gm, n, LLL, KKK) += DII * Y;
-                                                O(Gm, n, III, III) += 2.0 * DKJ * Y;
-                                                O(Gm, n, KKK, III) -= hx * 0.5 * DKI * Y;
-                                                O(Gm, n, LLL, III) -= hx * 0.5 * DJI * Y;
+                                                O(Gm, n, LLL, KKK) += J(III, III) * Y;
+                                                O(Gm, n, III, III) += 2.0 * J(LLL, KKK) * Y;
+                                                O(Gm, n, KKK, III) -= hx * 0.5 * K(LLL, III) * Y;
+                                                O(Gm, n, LLL, III) -= hx * 0.5 * K(KKK, III) * Y;
                                             }
                                         } else if (JJJ <= LLL) {
                                             double Y = hrrwhole(III, JJJ, KKK, LLL);
                                             if (C.gpu_screens && !(std::fabs(Y) > C.integralCutoff)) continue;
                                             if (III == JJJ && III == KKK && III == LLL) {
-                                                double DII = Dn(D, n, III, III);
-                                                O(Gm, n, III, III) += DII * Y - hx * 0.5 * DII * Y;
+                                                O(Gm, n, III, III) += J(III, III) * Y - hx * 0.5 * K(III, III) * Y;
                                             } else if (III == JJJ && III == KKK && III < LLL) {
-                                                double DJI = Dn(D, n, LLL, III), DII = Dn(D, n, III, III);
-                                                O(Gm, n, LLL, III) += DII * Y - hx * 0.5 * DII * Y;
-                                                O(Gm, n, III, III) += 2.0 * DJI * Y - hx * DJI * Y;
+                                                O(Gm, n, LLL, III) += J(III, III) * Y - hx * 0.5 * K(III, III) * Y;
+                                                O(Gm, n, III, III) += 2.0 * J(LLL, III) * Y - hx * K(LLL, III) * Y;
                                             } else if (III == KKK && JJJ == LLL && III < JJJ) {
-                                                double DJI = Dn(D, n, JJJ, III), DJJ = Dn(D, n, JJJ, JJJ), DII = Dn(D, n, III, III);
-                                                O(Gm, n, JJJ, III) += 2.0 * DJI * Y - hx * 0.5 * DJI * Y;
-                                                O(Gm, n, JJJ, JJJ) -= hx * 0.5 * DII * Y;
-                                                O(Gm, n, III, III) -= hx * 0.5 * DJJ * Y;
+                                                O(Gm, n, JJJ, III) += 2.0 * J(JJJ, III) * Y - hx * 0.5 * K(JJJ, III) * Y;
+                                                O(Gm, n, JJJ, JJJ) -= hx * 0.5 * K(III, III) * Y;
+                                                O(Gm, n, III, III) -= hx * 0.5 * K(JJJ, JJJ) * Y;
                                             } else if (III == KKK && III < JJJ && JJJ < LLL) {
-                                                double DKI = Dn(D, n, LLL, III), DKJ = Dn(D, n, LLL, JJJ);
-                                                double DII = Dn(D, n, III, III), DJI = Dn(D, n, JJJ, III);
-                                                O(Gm, n, JJJ, III) += 2.0 * DKI * Y - hx * 0.5 * DKI * Y;
-                                                O(Gm, n, LLL, III) += 2.0 * DJI * Y - hx * 0.5 * DJI * Y;
-                                                O(Gm, n, III, III) -= hx * 1.0 * DKJ * Y;
-                                                O(Gm, n, LLL, JJJ) -= hx * 0.5 * DII * Y;
+                                                O(Gm, n, JJJ, III) += 2.0 * J(LLL, III) * Y - hx * 0.5 * K(LLL, III) * Y;
+                                                O(Gm, n, LLL, III) += 2.0 * J(JJJ, III) * Y - hx * 0.5 * K(JJJ, III) * Y;
+                                                O(Gm, n, III, III) -= hx * 1.0 * K(LLL, JJJ) * Y;
+                                                O(Gm, n, LLL, JJJ) -= hx * 0.5 * K(III, III) * Y;
                                             }
                                         }
                                     }
@@ -814,15 +807,68 @@ void orc_density_cutoff(void* hv, const double* dense, double* cutmatrix) {
 // quartets evaluated.  Bra shells II = ii_begin, ii_begin + ii_stride, ... < ii_end
 // only (a bounded sample when the range is partial).  nthreads <= 0 uses the
 // OpenMP default.
+long long get2e_core(void* hv, const double* dense, const double* dense_k, const double* cutmatrix,
+                     const double* Ycutoff, const double* cutprim, double integralCutoff, double primLimit, double* o,
+                     int ii_begin, int ii_end, int nthreads, int ii_stride, int gpu_screens);
+
 long long orc_get2e(void* hv, const double* dense, const double* cutmatrix, const double* Ycutoff,
                     const double* cutprim, double integralCutoff, double primLimit, double* o,
                     int ii_begin, int ii_end, int nthreads, int ii_stride, int gpu_screens) {
+    return get2e_core(hv, dense, nullptr, cutmatrix, Ycutoff, cutprim, integralCutoff, primLimit, o, ii_begin,
+                      ii_end, nthreads, ii_stride, gpu_screens);
+}
+
+// Open-shell (UHF) build, get_oshell_eri (src/modules/include/eri.fh under OSHELL):
+// oa += J[Da + Db] - K[Da], ob += J[Da + Db] - K[Db] on the quartets the open-shell
+// density screen `cutmatrix` admits.  Each matrix is the closed-shell digestion with
+// J read from Da + Db and K from 2 Da (2 Db).  Returns the quartets evaluated.
+long long orc_get2e_uhf(void* hv, const double* Da, const double* Db, const double* cutmatrix,
+                        const double* Ycutoff, const double* cutprim, double integralCutoff, double primLimit,
+                        double* oa, double* ob, int nthreads) {
+    Basis& B = ((OracleHandle*)hv)->B;
+    const size_t nn = (size_t)B.nbasis * B.nbasis;
+    std::vector<double> Dt(nn), Ka(nn), Kb(nn);
+    for (size_t i = 0; i < nn; ++i) {
+        Dt[i] = Da[i] + Db[i];
+        Ka[i] = 2.0 * Da[i];
+        Kb[i] = 2.0 * Db[i];
+    }
+    long long nq = get2e_core(hv, Dt.data(), Ka.data(), cutmatrix, Ycutoff, cutprim, integralCutoff, primLimit, oa, 0,
+                              0, nthreads, 1, 0);
+    get2e_core(hv, Dt.data(), Kb.data(), cutmatrix, Ycutoff, cutprim, integralCutoff, primLimit, ob, 0, 0, nthreads, 1, 0);
+    return nq;
+}
+
+// QUICK's open-shell density screen (oshell_density_cutoff, src/modules/include/cutoff.fh:15-92):
+// per shell pair the largest of |Da + Db|, |Da|, |Db| over its block.
+void orc_density_cutoff_uhf(void* hv, const double* Da, const double* Db, double* cutmatrix) {
+    Basis& B = ((OracleHandle*)hv)->B;
+    int n = B.nbasis, ns = B.nshell;
+    for (int II = 0; II < ns; ++II)
+        for (int JJ = II; JJ < ns; ++JJ) {
+            double dn = 0.0;
+            int i1 = B.ksumtype[II] + B.qs(II, B.qstart[II]), i2 = B.ksumtype[II] + B.qf(II, B.qfinal[II]);
+            int j1 = B.ksumtype[JJ] + B.qs(JJ, B.qstart[JJ]), j2 = B.ksumtype[JJ] + B.qf(JJ, B.qfinal[JJ]);
+            for (int i = i1; i <= i2; ++i)
+                for (int j = j1; j <= j2; ++j) {
+                    const size_t k = (size_t)(j - 1) + (size_t)n * (i - 1);
+                    dn = std::max({dn, std::fabs(Da[k] + Db[k]), std::fabs(Da[k]), std::fabs(Db[k])});
+                }
+            cutmatrix[II + (size_t)ns * JJ] = dn;
+            cutmatrix[JJ + (size_t)ns * II] = dn;
+        }
+}
+
+long long get2e_core(void* hv, const double* dense, const double* dense_k, const double* cutmatrix,
+                     const double* Ycutoff, const double* cutprim, double integralCutoff, double primLimit, double* o,
+                     int ii_begin, int ii_end, int nthreads, int ii_stride, int gpu_screens) {
     Basis& B = ((OracleHandle*)hv)->B;
     int n = B.nbasis, ns = B.nshell;
     if (ii_end <= 0 || ii_end > ns) ii_end = ns;
     if (ii_stride <= 0) ii_stride = 1;
     const int nII = (ii_end - ii_begin + ii_stride - 1) / ii_stride;
     Ctx C{&B, dense, cutmatrix, cutprim, integralCutoff, primLimit};
+    C.dense_k = dense_k;
     C.gpu_screens = gpu_screens != 0;
     const double pair_cut = C.gpu_screens ? 1e-10 : -1.0;
     std::vector<double> G((size_t)n * n, 0.0);

@@ -71,6 +71,9 @@ def lib():
         L.orc_get2e.restype = ctypes.c_longlong
         L.orc_get2e.argtypes = [P, P, P, P, P, D, D, P, I, I, I, I, I]
         L.orc_oei.argtypes = [I, I, P, P, P, P, P, P, I, P, P, P, P, P]
+        L.orc_get2e_uhf.restype = ctypes.c_longlong
+        L.orc_get2e_uhf.argtypes = [P, P, P, P, P, P, D, D, P, P, I]
+        L.orc_density_cutoff_uhf.argtypes = [P, P, P, P]
         _lib = L
     return _lib
 
@@ -158,6 +161,31 @@ class Oracle:
                              int(ii_range[0]), int(ii_range[1]), int(nthreads), int(ii_stride),
                              int(bool(gpu_screens)))
         return out, nq
+
+
+def _uhf_methods():
+    def density_cutoff_uhf(self, Da, Db):
+        """QUICK's open-shell density screen (max of |Da + Db|, |Da|, |Db| per shell pair)."""
+        b = self.b
+        cm = np.zeros((b.nshell, b.nshell), order="F")
+        lib().orc_density_cutoff_uhf(self.h, _p(_f64(Da)), _p(_f64(Db)), _p(cm))
+        return cm
+
+    def get2e_uhf(self, Da, Db, cutmatrix, Ycut, cutprim, integral_cutoff, prim_limit, nthreads=0):
+        """(G_alpha, G_beta, quartet count) of the open-shell build (eri.fh under OSHELL)."""
+        b = self.b
+        oa = np.zeros((b.nbasis, b.nbasis), order="F")
+        ob = np.zeros((b.nbasis, b.nbasis), order="F")
+        nq = lib().orc_get2e_uhf(self.h, _p(_f64(Da)), _p(_f64(Db)), _p(_f64(cutmatrix)), _p(_f64(Ycut)),
+                                 _p(_f64(cutprim)), float(integral_cutoff), float(prim_limit), _p(oa), _p(ob),
+                                 int(nthreads))
+        return oa, ob, nq
+
+    Oracle.density_cutoff_uhf = density_cutoff_uhf
+    Oracle.get2e_uhf = get2e_uhf
+
+
+_uhf_methods()
 
 
 def oei(basis, ext_charges=None):
@@ -266,3 +294,72 @@ def rhf(basis, integral_cutoff=1e-11, prim_limit=1e-12, conv=1e-9, maxiter=100, 
             D = D_prev
             break
     return dict(E=Eel + Ecore, Eel=Eel, Ecore=Ecore, D=D, F=F, H=H, S=S, niter=it)
+
+
+def uhf(basis, mult, integral_cutoff=1e-11, prim_limit=1e-12, conv=1e-9, maxiter=200, nthreads=0,
+        fock_builder=None, guess="core"):
+    """Unrestricted (Pople-Nesbet) SCF with QUICK's open-shell Fock build; returns
+    dict(E, Da, Db, niter).  ``fock_builder(Da, Db, cutmatrix) -> (Ga, Gb)`` may
+    replace the oracle's get2e_uhf.  Energy: (tr[(Da + Db) H] + tr[Da Fa] + tr[Db Fb]) / 2
+    plus the nuclear repulsion; Pulay DIIS on the stacked alpha and beta commutators
+    (the reference's uscf, src/modules/quick_uscf_module.f90, in its essentials)."""
+    b = basis
+    S, T, V = oei(b)
+    H = T + V
+    X = orthogonalizer(S)
+    nel = b.mol.nelec
+    na, nb = (nel + mult - 1) // 2, (nel - mult + 1) // 2
+    orc = Oracle(b)
+    Ycut, cutprim = orc.schwarz(nthreads)
+
+    def G_of(Da, Db):
+        cm = orc.density_cutoff_uhf(Da, Db)
+        if fock_builder is not None:
+            return fock_builder(Da, Db, cm)
+        Ga, Gb, _ = orc.get2e_uhf(Da, Db, cm, Ycut, cutprim, integral_cutoff, prim_limit, nthreads)
+        return Ga, Gb
+
+    def dens(F, nocc):
+        e, C = np.linalg.eigh(X.T @ F @ X)
+        C = X @ C
+        return C[:, :nocc] @ C[:, :nocc].T
+
+    Da, Db = dens(H, na), dens(H, nb)
+    Ecore = b.mol.nuclear_repulsion()
+    errs, focks = [], []
+    E_old = 0.0
+    for it in range(1, maxiter + 1):
+        Ga, Gb = G_of(Da, Db)
+        Fa, Fb = H + Ga, H + Gb
+        Eel = 0.5 * float(np.sum((Da + Db) * H) + np.sum(Da * Fa) + np.sum(Db * Fb))
+        ea = X.T @ (Fa @ Da @ S - S @ Da @ Fa) @ X
+        eb = X.T @ (Fb @ Db @ S - S @ Db @ Fb) @ X
+        errs.append((ea, eb))
+        focks.append((Fa, Fb))
+        if len(errs) > 10:
+            errs.pop(0)
+            focks.pop(0)
+        nd = len(errs)
+        Bm = -np.ones((nd + 1, nd + 1))
+        Bm[nd, nd] = 0.0
+        for i in range(nd):
+            for j in range(nd):
+                Bm[i, j] = float(np.sum(errs[i][0] * errs[j][0]) + np.sum(errs[i][1] * errs[j][1]))
+        rhs = np.zeros(nd + 1)
+        rhs[nd] = -1.0
+        try:
+            c = np.linalg.solve(Bm, rhs)[:nd]
+            Fa_d = sum(ci * f[0] for ci, f in zip(c, focks))
+            Fb_d = sum(ci * f[1] for ci, f in zip(c, focks))
+        except np.linalg.LinAlgError:
+            Fa_d, Fb_d = Fa, Fb
+        Dan, Dbn = dens(Fa_d, na), dens(Fb_d, nb)
+        dmax = max(float(np.abs(Dan - Da).max()), float(np.abs(Dbn - Db).max()))
+        converged = dmax < conv and abs(Eel - E_old) < 1e-10
+        Da_prev, Db_prev = Da, Db
+        Da, Db = Dan, Dbn
+        E_old = Eel
+        if converged:
+            Da, Db = Da_prev, Db_prev
+            break
+    return dict(E=Eel + Ecore, Eel=Eel, Ecore=Ecore, Da=Da, Db=Db, niter=it)

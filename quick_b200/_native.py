@@ -25,6 +25,7 @@ EXPORTED = [
     "qk_last_work_mixed", "qk_batch_create", "qk_batch_destroy", "qk_batch_fock2e",
     "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_sp2_step", "qk_set_shard", "qk_fock2e_device_accumulate", "qk_finalize_fixed", "qk_set_streams",
     "qk_set_class_launch", "qk_class_launch", "qk_batch_reserve_sms", "qk_boys", "qk_set_boys", "qk_set_worklist_builder",
+    "gpu_upload_calculated_beta_", "gpu_get_oshell_eri_", "qk_fock2e_uhf_device", "qk_fock2e_uhf_host",
 ]
 
 _lib = None
@@ -63,6 +64,8 @@ def lib():
     L.qk_boys.argtypes = [P, I, P, I, P, P]
     L.qk_set_boys.argtypes = [P, I]
     L.qk_set_worklist_builder.argtypes = [P, I]
+    L.qk_fock2e_uhf_device.argtypes = [P, P, P, P, P, P, P]
+    L.qk_fock2e_uhf_host.argtypes = [P, P, P, P, P, P]
     L.qk_fock2e_host.argtypes = [P, P, P, P]
     L.qk_density_cutoff_device.argtypes = [P, P, P, P]
     L.qk_last_work.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), PI]

@@ -76,6 +76,7 @@ struct DevData {
     unsigned long long* stats;           // optional: [quartets computed, primitive quartets computed]
     double cut, primLimit;
     int boys_mode;                       // qk_set_boys: 0 accurate; 1 QUICK CPU order; 2 QUICK GPU order
+    int exchange_only;                   // 1: the K part alone (the spin-density half of a UHF build)
 };
 
 __device__ __forceinline__ void atomic_fixed(unsigned long long* addr, double v) {
@@ -207,8 +208,8 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
     const int fa = d.q_f0[qa], fb = d.q_f0[qb], fc = d.q_f0[qc], fd = d.q_f0[qd];
     // degeneracy of the unique quartet (pairs are unordered, bra/ket unordered)
     const double deg = (qa != qb ? 2.0 : 1.0) * (qc != qd ? 2.0 : 1.0) * (P != Q ? 2.0 : 1.0);
-    const double wJ = 0.25 * deg;      // 2 * deg/8
-    const double wK = -0.0625 * deg;   // -1/2 * deg/8
+    const double wJ = d.exchange_only ? 0.0 : 0.25 * deg;   // 2 * deg/8
+    const double wK = -0.0625 * deg;                        // -1/2 * deg/8
 
     double Dab[NAB], Dcd[NC * ND], Dbd[NB * ND], Dad[NA * ND], Dbc[NB * NC], Dac[NA * NC];
 #pragma unroll
@@ -274,10 +275,12 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
         }
     }
     unsigned long long* A = d.A;
+    if (!d.exchange_only) {
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+        for (int c = 0; c < NC; ++c)
 #pragma unroll
-        for (int e = 0; e < ND; ++e) atomic_fixed(A + (size_t)(fc + c) * n + fd + e, wJ * jcd[c * ND + e]);
+            for (int e = 0; e < ND; ++e) atomic_fixed(A + (size_t)(fc + c) * n + fd + e, wJ * jcd[c * ND + e]);
+    }
 #pragma unroll
     for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -507,12 +510,14 @@ __device__ __forceinline__ void coop_quartet(const DevData& d, int P, int Q, dou
     const double wJ = 0.25 * deg, wK = -0.0625 * deg;
     unsigned long long* A = d.A;
     // J over the bra: (ab) row . Dcd;  J over the ket: (cd) column . Dab
-    digest_group<NAB, NC, ND, ND, 1>(
-        lane, wJ, A, I, Dcd, [&](int ab) { return ab * NCD; },
-        [&](int ab) { return (size_t)(fa + ab / NB) * n + fb + ab % NB; });
-    digest_group<NCD, NA, NB, NB * NCD, NCD>(
-        lane, wJ, A, I, Dab, [&](int cd) { return cd; },
-        [&](int cd) { return (size_t)(fc + cd / ND) * n + fd + cd % ND; });
+    if (!d.exchange_only) {   // warp-uniform
+        digest_group<NAB, NC, ND, ND, 1>(
+            lane, wJ, A, I, Dcd, [&](int ab) { return ab * NCD; },
+            [&](int ab) { return (size_t)(fa + ab / NB) * n + fb + ab % NB; });
+        digest_group<NCD, NA, NB, NB * NCD, NCD>(
+            lane, wJ, A, I, Dab, [&](int cd) { return cd; },
+            [&](int cd) { return (size_t)(fc + cd / ND) * n + fd + cd % ND; });
+    }
     // K_ac = sum_bd I D_bd,  K_bc = sum_ad I D_ad,  K_ad = sum_bc I D_bc,  K_bd = sum_ac I D_ac
     digest_group<NA * NC, NB, ND, NCD, 1>(
         lane, wK, A, I, Dbd, [&](int ac) { return (ac / NC) * NB * NCD + (ac % NC) * ND; },
@@ -599,6 +604,7 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
                 atomicAdd(d.stats + 1, (unsigned long long)sp);
             }
         }
+        if (d.exchange_only) continue;   // no J part
         const int P = w.x;
         const int qa = d.pr_qa[P], qb = d.pr_qb[P];
         const int fa = d.q_f0[qa], fb = d.q_f0[qb];
@@ -655,6 +661,7 @@ fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restri
         for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
         int nq = 0, np = 0;
         if (lane < w.z) fock_quartet<La, Lb, Lc, Ld, FP32>(d, bt, w.x, w.y + lane, jab, &nq, &np);
+        if (d.exchange_only) continue;
         const int P = w.x;
         const int fa = d.q_f0[d.pr_qa[P]], fb = d.q_f0[d.pr_qb[P]];
 #pragma unroll
@@ -927,6 +934,46 @@ static cudaError_t launch_boys_probe(const double* T, int n, const double2* rows
     return cudaGetLastError();
 }
 
+// Open shell (UHF): total and spin densities Dt = Da + Db, Ds = Da - Db.
+__global__ void uhf_densities_kernel(const double* __restrict__ Da, const double* __restrict__ Db, long long nn,
+                                     double* __restrict__ Dt, double* __restrict__ Ds) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (long long)gridDim.x * blockDim.x) {
+        const double a = Da[t], b = Db[t];
+        Dt[t] = a + b;
+        Ds[t] = a - b;
+    }
+}
+
+// QUICK's open-shell density screen (oshell_density_cutoff, src/modules/include/cutoff.fh:15-92):
+// per shell pair the largest of |Da + Db|, |Da|, |Db| over its block.
+__global__ void density_cutoff_uhf_kernel(const double* __restrict__ Da, const double* __restrict__ Db, int n,
+                                          int nshell, const int* __restrict__ s_f0, const int* __restrict__ s_f1,
+                                          double* __restrict__ cutmat) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nshell * nshell) return;
+    const int a = t / nshell, b = t % nshell;
+    double m = 0.0;
+    for (int i = s_f0[a]; i < s_f1[a]; ++i)
+        for (int j = s_f0[b]; j < s_f1[b]; ++j) {
+            const double x = Da[(size_t)j * n + i], y = Db[(size_t)j * n + i];
+            m = fmax(m, fmax(fabs(x + y), fmax(fabs(x), fabs(y))));
+        }
+    cutmat[t] = m;
+}
+
+// oa += G_cs(Dt) + K(Ds), ob += G_cs(Dt) - K(Ds): A1 the closed-shell build of Dt,
+// A2 the exchange-only build of Ds (both int64 fixed point; sums taken exactly).
+__global__ void finalize_uhf_kernel(const unsigned long long* __restrict__ A1, const unsigned long long* __restrict__ A2,
+                                    int n, double* __restrict__ oa, double* __restrict__ ob) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * n) return;
+    const int i = t / n, j = t % n;
+    const size_t ij = (size_t)i * n + j, ji = (size_t)j * n + i;
+    const unsigned long long j1 = A1[ij] + A1[ji], k2 = A2[ij] + A2[ji];
+    oa[t] += (double)(long long)(j1 + k2) * kFixedInv;
+    ob[t] += (double)(long long)(j1 - k2) * kFixedInv;
+}
+
 __global__ void finalize_kernel(const unsigned long long* __restrict__ A, int n, double* __restrict__ o) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n * n) return;
@@ -1117,7 +1164,8 @@ struct qk_ctx {
     // device buffers
     qk::DevBuf<double> d_xyz, d_boys, d_boys8, d_D, d_cutmat, d_o;
     qk::DevBuf<int> d_q_atom, d_q_f0, d_q_parent, d_q_ltop, d_q_prim0, d_q_nprim, d_shell_f0, d_shell_f1;
-    qk::DevBuf<unsigned long long> d_A;
+    qk::DevBuf<unsigned long long> d_A, d_A2;   // d_A2: the exchange-only half of a UHF build
+    qk::DevBuf<double> d_uhf;                     // UHF: Dt and Ds (2 nbasis^2), then Db and ob for host calls
     qk::DevBuf<int> d_counters;
     // optional per-class timing (CUDA events on the launching stream) and work counters
     bool profile_events = false, profile_stats = false;
@@ -1134,7 +1182,8 @@ struct qk_ctx {
     std::vector<int> launch_order;   // class indices, coop classes first, then by listed work
     // drop-in (reference-shaped) state
     std::vector<double> host_D, host_cutmat;
-    bool have_D = false, have_cutmat = false;
+    std::vector<double> host_Db;            // beta density (gpu_upload_calculated_beta_)
+    bool have_D = false, have_Db = false, have_cutmat = false;
 };
 
 namespace qk {
@@ -1751,7 +1800,7 @@ static void launch_class(const ClassEntry& ce, const ClassWork& W, cudaStream_t 
 // instead of the context's, for sharded builds whose accumulators are summed
 // across GPUs before the one finalisation; o is then unused.
 static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, double* o, cudaStream_t s,
-                         unsigned long long* A_ext = nullptr) {
+                         unsigned long long* A_ext = nullptr, int exchange_only = 0) {
     // a sharded context holds only its share of the work: finalising that share
     // into o would be a silently partial Fock matrix
     if (!A_ext && c->shard_count > 1)
@@ -1777,6 +1826,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     d.cutmat = cutmat;
     d.A = A_ext ? A_ext : c->d_A.p;
     d.stats = nullptr;
+    d.exchange_only = exchange_only;
     if (c->profile_stats) {
         QK_CUDA_TRY(c->d_stats.reserve(2 * kNumClasses));
         QK_CUDA_TRY(cudaMemsetAsync(c->d_stats.p, 0, sizeof(unsigned long long) * 2 * kNumClasses, s));
@@ -1829,6 +1879,45 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     return QK_OK;
 }
 
+
+// Open-shell (UHF) Fock build: oa += G_a, ob += G_b with G_a = J[Da + Db] - K[Da],
+// G_b = J[Da + Db] - K[Db] (QUICK's get_oshell_eri, src/modules/include/eri.fh under
+// OSHELL; src/gpu/gpu_get2e_subs.h:638-660).  Written as one closed-shell build of the
+// total density Dt = Da + Db (J - K/2) and one exchange-only build of the spin density
+// Ds = Da - Db (-K/2): G_a = G(Dt) + K(Ds), G_b = G(Dt) - K(Ds).  Both builds use the
+// open-shell density screen, so their quartets are QUICK's open-shell set.
+static int fock2e_uhf_device(qk_ctx* c, const double* Da, const double* Db, const double* cutmat, double* oa,
+                             double* ob, cudaStream_t s) {
+    if (c->shard_count > 1)
+        return fail(QK_ERR_INVALID_ARG, "context is sharded (qk_set_shard): UHF builds are not sharded");
+    int st = ensure_pairs(c);
+    if (st) return st;
+    const int n = c->nbasis, ns = c->nshell;
+    const size_t nn = (size_t)n * n;
+    QK_CUDA_TRY(c->d_uhf.reserve(2 * nn));
+    double* Dt = c->d_uhf.p;
+    double* Ds = c->d_uhf.p + nn;
+    uhf_densities_kernel<<<(int)std::min<size_t>((nn + 255) / 256, 8192), 256, 0, s>>>(Da, Db, (long long)nn, Dt, Ds);
+    QK_CUDA_TRY(cudaGetLastError());
+    if (!cutmat) {
+        QK_CUDA_TRY(c->d_cutmat.reserve((size_t)ns * ns));
+        density_cutoff_uhf_kernel<<<(ns * ns + 127) / 128, 128, 0, s>>>(Da, Db, n, ns, c->d_shell_f0.p,
+                                                                        c->d_shell_f1.p, c->d_cutmat.p);
+        QK_CUDA_TRY(cudaGetLastError());
+        cutmat = c->d_cutmat.p;
+    }
+    QK_CUDA_TRY(c->d_A.reserve(nn));
+    QK_CUDA_TRY(c->d_A2.reserve(nn));
+    QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * nn, s));
+    QK_CUDA_TRY(cudaMemsetAsync(c->d_A2.p, 0, sizeof(unsigned long long) * nn, s));
+    st = fock2e_device(c, Dt, cutmat, nullptr, s, c->d_A.p, 0);
+    if (st) return st;
+    st = fock2e_device(c, Ds, cutmat, nullptr, s, c->d_A2.p, 1);
+    if (st) return st;
+    finalize_uhf_kernel<<<(int)((nn + 255) / 256), 256, 0, s>>>(c->d_A.p, c->d_A2.p, n, oa, ob);
+    QK_CUDA_TRY(cudaGetLastError());
+    return QK_OK;
+}
 
 // ------------------------------------------------------------------ fixed scratch
 // Scratch of the allocation-free build (qk_fock2e_device_noalloc).  Some callers
@@ -2313,6 +2402,42 @@ int qk_fock2e_host(qk_ctx* c, const double* D, const double* cutmat, double* o) 
     return QK_OK;
 }
 
+int qk_fock2e_uhf_device(qk_ctx* c, const double* Da, const double* Db, const double* cutmat, double* oa, double* ob,
+                         void* stream) {
+    if (!c || !Da || !Db || !oa || !ob) return fail(QK_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    return fock2e_uhf_device(c, Da, Db, cutmat, oa, ob, (cudaStream_t)stream);
+}
+
+int qk_fock2e_uhf_host(qk_ctx* c, const double* Da, const double* Db, const double* cutmat, double* oa, double* ob) {
+    if (!c || !Da || !Db || !oa || !ob) return fail(QK_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> g(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice");
+    const int n = c->nbasis, ns = c->nshell;
+    const size_t nn = (size_t)n * n;
+    cudaStream_t s = c->stream;
+    // device copies: Da in d_D, oa in d_o, Db and ob in the second half of d_D / d_o
+    QK_CUDA_TRY(c->d_D.reserve(2 * nn));
+    QK_CUDA_TRY(c->d_o.reserve(2 * nn));
+    QK_CUDA_TRY(cudaMemcpyAsync(c->d_D.p, Da, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(c->d_D.p + nn, Db, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(c->d_o.p, oa, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(c->d_o.p + nn, ob, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+    const double* cm = nullptr;
+    if (cutmat) {
+        QK_CUDA_TRY(c->d_cutmat.reserve((size_t)ns * ns));
+        QK_CUDA_TRY(cudaMemcpyAsync(c->d_cutmat.p, cutmat, sizeof(double) * ns * ns, cudaMemcpyHostToDevice, s));
+        cm = c->d_cutmat.p;
+    }
+    int st = fock2e_uhf_device(c, c->d_D.p, c->d_D.p + nn, cm, c->d_o.p, c->d_o.p + nn, s);
+    if (st) return st;
+    QK_CUDA_TRY(cudaMemcpyAsync(oa, c->d_o.p, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaMemcpyAsync(ob, c->d_o.p + nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
+    QK_CUDA_TRY(cudaStreamSynchronize(s));
+    return QK_OK;
+}
+
 // Allocation-free variant of qk_fock2e_device for callers that may not allocate
 // device memory when they run a Fock build; see the comment at g_noalloc_scratch.
 // Its first call on a device looks up the scratch array's device address (one
@@ -2564,7 +2689,7 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
                      T.d_payz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
                      c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(), c->d_q_ltop.bytes(),
                      c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
-                     c->d_A.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
+                     c->d_A.bytes(), c->d_A2.bytes(), c->d_uhf.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
         t += b;
     if (total) *total = t;
     if (items) *items = it;
@@ -2771,9 +2896,9 @@ void gpu_setup_(int* natom, int* nbasis, int*, int*, int*, int*) {
     c->nbasis = *nbasis;
 }
 
-void gpu_upload_method_(int* method, bool* is_oshell, double*) {
-    if (!method || *method != 0 || (is_oshell && *is_oshell))
-        fail(QK_ERR_UNSUPPORTED, "only closed-shell HF exchange is implemented");
+void gpu_upload_method_(int* method, bool*, double*) {
+    // closed and open shell (gpu_get_cshell_eri_ / gpu_get_oshell_eri_) with HF exchange
+    if (!method || *method != 0) fail(QK_ERR_UNSUPPORTED, "only HF exchange (method 0) is implemented");
 }
 
 void gpu_upload_xyz_(double* atom_xyz) {
@@ -2822,6 +2947,20 @@ void gpu_get_cshell_eri_(bool*, double* o) {
     // the density (or delta density when deltaO) arrives through gpu_upload_calculated_,
     // exactly as in the reference; deltaO only changes what the caller uploaded
     qk_fock2e_host(c, c->host_D.data(), c->have_cutmat ? c->host_cutmat.data() : nullptr, o);
+}
+
+void gpu_upload_calculated_beta_(double*, double* denseb) {
+    qk_ctx* c = qk_default_ctx();
+    if (!c || !denseb) { fail(QK_ERR_INVALID_ARG, "gpu_upload_calculated_beta_"); return; }
+    c->host_Db.assign(denseb, denseb + (size_t)c->nbasis * c->nbasis);
+    c->have_Db = true;
+}
+
+void gpu_get_oshell_eri_(bool*, double* o, double* ob) {
+    qk_ctx* c = qk_default_ctx();
+    if (!c || !o || !ob) { fail(QK_ERR_INVALID_ARG, "gpu_get_oshell_eri_"); return; }
+    if (!c->have_D || !c->have_Db) { fail(QK_ERR_NOT_READY, "gpu_get_oshell_eri_: densities not uploaded"); return; }
+    qk_fock2e_uhf_host(c, c->host_D.data(), c->host_Db.data(), c->have_cutmat ? c->host_cutmat.data() : nullptr, o, ob);
 }
 
 void gpu_delete_(int* ierr) {

@@ -146,6 +146,26 @@ class Get2e:
                                              ctypes.c_void_p(stream.cuda_stream)), "qk_density_cutoff_device")
         return out
 
+    def fock2e_uhf(self, Da, Db, oa=None, ob=None, cutmat=None, stream=None):
+        """Open-shell build: oa += G_alpha(Da, Db), ob += G_beta(Da, Db) on the device
+        (CUDA float64 tensors); returns (oa, ob).  ``cutmat``: the open-shell density
+        screen, or None to derive it from Da and Db."""
+        import torch
+        n = self.basis.nbasis
+        for X in (Da, Db):
+            if X.dtype != torch.float64 or not X.is_cuda or tuple(X.shape) != (n, n):
+                raise ValueError("Da and Db must be CUDA float64 tensors of shape (nbasis, nbasis)")
+        Da, Db = Da.contiguous(), Db.contiguous()
+        oa = torch.zeros_like(Da) if oa is None else oa
+        ob = torch.zeros_like(Db) if ob is None else ob
+        if stream is None:
+            stream = torch.cuda.current_stream(Da.device)
+        cm = ctypes.c_void_p(cutmat.data_ptr()) if cutmat is not None else None
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        check(lib().qk_fock2e_uhf_device(self.h, vp(Da), vp(Db), cm, vp(oa), vp(ob),
+                                         ctypes.c_void_p(stream.cuda_stream)), "qk_fock2e_uhf_device")
+        return oa, ob
+
     def fock2e_host(self, D, o=None, cutmat=None):
         """Host arrays: returns o + G(D) (copies in, computes, copies out)."""
         n = self.basis.nbasis
@@ -375,6 +395,19 @@ def gpu_get_cshell_eri(deltaO, o):
     if not (isinstance(o, np.ndarray) and o.dtype == np.float64 and o.flags.f_contiguous):
         raise ValueError("o must be a Fortran-ordered float64 array")
     lib().gpu_get_cshell_eri_(_ref(bool(deltaO), _c_bool), _p(o))
+
+
+def gpu_upload_calculated_beta(ob, denseb):
+    ob, denseb = _f64(ob), _f64(denseb)
+    lib().gpu_upload_calculated_beta_(_p(ob), _p(denseb))
+
+
+def gpu_get_oshell_eri(deltaO, o, ob):
+    """o += G_alpha, ob += G_beta (Fortran-ordered float64 arrays, modified in place)."""
+    for a in (o, ob):
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.f_contiguous):
+            raise ValueError("o and ob must be Fortran-ordered float64 arrays")
+    lib().gpu_get_oshell_eri_(_ref(bool(deltaO), _c_bool), _p(o), _p(ob))
 
 
 def gpu_delete():

@@ -5,7 +5,8 @@ source tree (keyword line, charge, geometry in Angstrom) and the saved output
 ``test/saved/<name>.out`` (``TOTAL ENERGY`` and ``ELECTRONIC ENERGY`` lines,
 printed with 9 decimals by ``src/getEnergy.f90:161-162``), plus the f-function
 RHF energy of ``grad_nma_rhf_def2tzvp`` (a CPU-build golden).  Only basis sets
-packaged under ``quick_b200/basis_data`` are kept.
+packaged under ``quick_b200/basis_data`` are kept.  The open-shell tests
+``test/*_uhf_*.in`` give ``uhf_energies.json`` (their first TOTAL ENERGY).
 
 Usage::
 
@@ -76,6 +77,30 @@ def main(root):
     with open(os.path.join(HERE, "rhf_energies.json"), "w") as f:
         json.dump(cases, f, indent=1)
     print(len(cases), "cases")
+    # open-shell: the UHF energy at the input geometry (the first TOTAL ENERGY line of
+    # the reference's only UHF regression output, a geometry optimisation)
+    uhf = []
+    for inp in sorted(glob.glob(os.path.join(root, "test", "*_uhf_*.in"))):
+        name = os.path.basename(inp)[:-3]
+        out = os.path.join(root, "test", "saved", name + ".out")
+        if not os.path.exists(out):
+            continue
+        kw, basis, charge, mult, atoms = parse_input(inp)
+        if basis not in PACKAGED or "DFT" in kw or "B3LYP" in kw:
+            continue
+        first = None
+        with open(out) as f:
+            for ln in f:
+                if "TOTAL ENERGY" in ln and "=" in ln:
+                    first = float(ln.split("=")[1].split()[0])
+                    break
+        if first is None:
+            continue
+        uhf.append({"name": name, "basis": basis, "charge": charge, "mult": mult, "atoms": atoms,
+                    "total_energy": first, "source": f"test/{name}.in, test/saved/{name}.out (step 1)"})
+    with open(os.path.join(HERE, "uhf_energies.json"), "w") as f:
+        json.dump(uhf, f, indent=1)
+    print(len(uhf), "UHF cases")
 
 
 if __name__ == "__main__":
