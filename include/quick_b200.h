@@ -254,6 +254,15 @@ int qk_launches_per_build(qk_ctx *ctx);
  * (gpu_upload_cutoff_matrix_, src/gpu/cuda/gpu.cu:879-1470). */
 int qk_set_worklist_builder(qk_ctx *ctx, int on_device);
 
+/* A stream of the caller's own: non-blocking, at the device's highest priority
+ * (high_priority != 0) or its lowest, owned by nobody else.  Streams handed out by a
+ * framework's pool may be shared with other threads; a thread that captures a CUDA
+ * graph needs one that no other thread can enqueue work on.  Free it with
+ * qk_stream_destroy once its work is done.  No reference counterpart (QUICK runs one
+ * SCF per process on the default stream). */
+int qk_stream_create(int device, int high_priority, void **stream);
+int qk_stream_destroy(void *stream);
+
 /* Launch shape of a build: the class kernels run concurrently over `nstreams`
  * auxiliary streams forked from the caller's stream (1..4, default 4), or one after
  * another on the caller's stream (0).  A tuning knob: which is faster depends on

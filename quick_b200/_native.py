@@ -26,6 +26,7 @@ EXPORTED = [
     "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_sp2_step", "qk_set_shard", "qk_fock2e_device_accumulate", "qk_finalize_fixed", "qk_set_streams",
     "qk_set_class_launch", "qk_class_launch", "qk_batch_reserve_sms", "qk_boys", "qk_set_boys", "qk_set_worklist_builder",
     "gpu_upload_calculated_beta_", "gpu_get_oshell_eri_", "qk_fock2e_uhf_device", "qk_fock2e_uhf_host",
+    "qk_stream_create", "qk_stream_destroy",
 ]
 
 _lib = None
@@ -64,6 +65,8 @@ def lib():
     L.qk_boys.argtypes = [P, I, P, I, P, P]
     L.qk_set_boys.argtypes = [P, I]
     L.qk_set_worklist_builder.argtypes = [P, I]
+    L.qk_stream_create.argtypes = [I, I, ctypes.POINTER(ctypes.c_void_p)]
+    L.qk_stream_destroy.argtypes = [P]
     L.qk_fock2e_uhf_device.argtypes = [P, P, P, P, P, P, P]
     L.qk_fock2e_uhf_host.argtypes = [P, P, P, P, P, P]
     L.qk_fock2e_host.argtypes = [P, P, P, P]
@@ -113,3 +116,21 @@ def status_string(status: int) -> str:
 def check(status: int, what: str = "quick_b200"):
     if status != 0:
         raise QuickError(status, what)
+
+
+def own_stream(device: int, high_priority: bool = True):
+    """A torch view of a stream created for the caller alone (qk_stream_create).
+
+    torch's ``torch.cuda.Stream`` hands out streams from a fixed pool per priority,
+    round robin, so two threads can be given the same stream; a thread that captures
+    a CUDA graph on a shared stream has its capture invalidated (or other work
+    captured into it) when another thread enqueues there.  Free the stream with
+    :func:`free_stream` after its work is done."""
+    import torch
+    p = ctypes.c_void_p()
+    check(lib().qk_stream_create(int(device), 1 if high_priority else 0, ctypes.byref(p)), "qk_stream_create")
+    return torch.cuda.ExternalStream(p.value, device=torch.device("cuda", int(device)))
+
+
+def free_stream(stream) -> None:
+    check(lib().qk_stream_destroy(ctypes.c_void_p(stream.cuda_stream)), "qk_stream_destroy")

@@ -271,6 +271,16 @@ def class_list(lmax=LMAX):
     return out
 
 
+# Register ceiling of each per-lane class kernel (__maxnreg__).  ptxas's own choice
+# for these kernels varies from build to build (psss got 80 registers in one build
+# and 103 in another, dpss 128 and 170) and the higher counts cost occupancy; the
+# ceilings below are the fastest of a sweep (no ceiling, 128, 85, 64 and the
+# allocations ptxas chose) measured on 32 H2O / 6-31G*, per class kernel timed
+# alone.  Classes not listed keep ptxas's choice (255 = no ceiling).
+LANE_REGS = {(0, 0, 0, 0): 64, (1, 0, 0, 0): 80, (2, 0, 0, 0): 96, (2, 1, 0, 0): 128, (2, 2, 0, 0): 128,
+             (1, 1, 1, 0): 128, (2, 0, 1, 0): 128}
+
+
 def emit_class(La, Lb, Lc, Ld):
     Lab, Lcd = La + Lb, Lc + Ld
     M = Lab + Lcd
@@ -347,6 +357,7 @@ def emit_class(La, Lb, Lc, Ld):
     o.append(f"  static __device__ __forceinline__ double cons_c(int i) {{ const double t[{nc}] = {{{cc}}}; return t[i]; }}")
     o.append(f"  static __device__ __forceinline__ double cons_d(int i) {{ const double t[{nd}] = {{{cd}}}; return t[i]; }}")
     o.append(f"  static constexpr bool COOP = {'true' if coop else 'false'};")
+    o.append(f"  static constexpr int LANE_REGS = {LANE_REGS.get((La, Lb, Lc, Ld), 255)};")
     if coop:
         rows, off, tslots = vrr_table(g, targets, M)
         o.append(f"  static constexpr int NNODE = {len(rows)}, NLEVEL = {len(off) - 1}, NSLOT = {M + 2 + len(rows)};")

@@ -570,8 +570,9 @@ __device__ __forceinline__ const double2* class_boys_rows(const double2* __restr
 }
 
 // Per-lane class kernels launch with 1..kMaxLaneWarps warps per block (default
-// kWarpsPerBlock; the autotuner picks per class).  The bound leaves the register
-// allocation as it is for 128-thread blocks (255 registers allowed either way).
+// kWarpsPerBlock; the autotuner picks per class).  Their register ceiling is the
+// class's LANE_REGS (gen_eri.py: measured per class; 255 = ptxas's own choice, which
+// 256-thread blocks can always launch).
 constexpr int kMaxLaneWarps = 8;
 
 // Work item: x = bra pair, y = first ket pair, z = number of kets (<= 32),
@@ -579,7 +580,7 @@ constexpr int kMaxLaneWarps = 8;
 // FP32 = true: the mixed form's small-bound items (VRR and contraction in FP32),
 // compiled apart so that the FP64 items keep their register budget and vice versa.
 template <int La, int Lb, int Lc, int Ld, bool FP32>
-__global__ void __launch_bounds__(32 * kMaxLaneWarps)
+__global__ void __maxnreg__((EriClass<La, Lb, Lc, Ld>::LANE_REGS))
 fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
     constexpr int NAB = Cls::NA * Cls::NB;
@@ -641,7 +642,7 @@ __device__ __forceinline__ int batch_find_seg(const BatchSeg* __restrict__ segs,
 }
 
 template <int La, int Lb, int Lc, int Ld, bool FP32>
-__global__ void __launch_bounds__(32 * kMaxLaneWarps)
+__global__ void __maxnreg__((EriClass<La, Lb, Lc, Ld>::LANE_REGS))
 fock_class_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restrict__ segs, int nseg, int n_items,
                         int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
@@ -2732,6 +2733,31 @@ int qk_class_launch(qk_ctx* c, int ci, int* warps_per_block, int* max_warps, int
     if (blocks_per_sm) *blocks_per_sm = c->cls_bpsm[ci];
     if (grid) *grid = W.n_items == 0 ? 0 : W.grid;
     return QK_OK;
+}
+
+int qk_stream_create(int device, int high_priority, void** stream) {
+    if (!stream) return fail(QK_ERR_INVALID_ARG, "qk_stream_create: stream is NULL");
+    *stream = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(QK_ERR_INVALID_ARG, "qk_stream_create: device index out of range");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return fail(QK_ERR_CUDA, "cudaSetDevice failed");
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high_priority ? hi : lo);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return fail(QK_ERR_CUDA, "qk_stream_create: stream creation failed");
+    *stream = s;
+    return QK_OK;
+}
+
+int qk_stream_destroy(void* stream) {
+    if (!stream) return QK_OK;
+    return cudaStreamDestroy(static_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? QK_OK : fail(QK_ERR_CUDA, "qk_stream_destroy failed");
 }
 
 int qk_set_worklist_builder(qk_ctx* c, int on_device) {

@@ -29,7 +29,7 @@ import time
 import numpy as np
 
 from . import _native
-from ._native import check, lib
+from ._native import check, lib, own_stream
 from .get2e import Get2e
 
 # QUICK's level-shift controls (quick_method_module.f90:96-98): allowed from cycle
@@ -588,10 +588,11 @@ class DeviceSCFState:
                 # one memory pool for every solve's graph (they replay one after
                 # another on one stream), owned by a small anchor graph that lives
                 # as long as the process: a pool dies with its last graph
-                # the capture stream comes from torch's high-priority stream pool:
-                # pool streams are shared, and a normal-priority one may be another
-                # thread's current stream
-                pool, cs = torch.cuda.graph_pool_handle(), torch.cuda.Stream(dev, priority=-1)
+                # the capture stream is this process's own (not one of torch's pool
+                # streams, which other threads can be handed too: their work would
+                # land in the capture); it lives as long as the pool
+                pool = torch.cuda.graph_pool_handle()
+                cs = own_stream(dev.index if dev.index is not None else torch.cuda.current_device())
                 x = torch.zeros(1, device=dev)
                 anchor = torch.cuda.CUDAGraph()
                 cs.wait_stream(main)

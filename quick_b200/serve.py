@@ -41,6 +41,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from ._native import free_stream, own_stream
 from .basis import A_TO_BOHRS, Molecule, build_basis
 from .molecules import water_cluster
 
@@ -282,6 +283,8 @@ class Server:
         (a @ a).sum().item()
         self.executor = ThreadPoolExecutor(max_workers=workers) if workers > 0 else None
         self._tls = threading.local()
+        self._own_streams = []        # the set-up threads' streams, freed by close()
+        self._streams_lock = threading.Lock()
         self.setting_up = []          # (future, request, reserved bytes, admission time)
 
     # -- admission
@@ -289,8 +292,11 @@ class Server:
         st = getattr(self._tls, "stream", None)
         if st is None:
             self.torch.cuda.set_device(self.device)
-            # high priority: the set-up's kernels get SMs at the batch kernels' boundaries
-            st = self._tls.stream = self.torch.cuda.Stream(self.device, priority=-1)
+            # high priority: the set-up's kernels get SMs at the batch kernels' boundaries;
+            # a stream of its own, never one that a graph capture may be using
+            st = self._tls.stream = own_stream(self.device)
+            with self._streams_lock:
+                self._own_streams.append(st)
         return st
 
     def _setup(self, req, eng, D0):
@@ -504,6 +510,11 @@ class Server:
         self.pool = []
         self.used = 0
         self.batch.close()
+        if self._own_streams:
+            self.torch.cuda.synchronize(self.device)
+            for st in self._own_streams:
+                free_stream(st)
+            self._own_streams = []
 
 
 def summarize(results, wall: float) -> dict:
