@@ -553,7 +553,7 @@ class DeviceSCFState:
     _pools = {}
 
     def __init__(self, rhf, denserms=1e-6, maxiter=100, guess="sad", ncyc=3, D0=None, maxdiis=10, g=None,
-                 graph: bool = False, adaptive_cutoff: bool = False):
+                 graph: bool = False, adaptive_cutoff: bool = False, lane: int = 0):
         self.rhf = rhf
         self.cutoffs = CutoffSchedule(rhf.eng, adaptive_cutoff)
         self.g = g if g is not None else GraphSCF(rhf, maxdiis=maxdiis)
@@ -561,6 +561,7 @@ class DeviceSCFState:
         # (one launch per solve and step instead of some hundred)
         self.use_graph = graph
         self.post_graph = None
+        self.lane = lane            # the stream and graph memory pool its post-build graph uses
         self.g.begin(guess, D0)
         self.denserms, self.maxiter, self.ncyc = denserms, maxiter, ncyc
         self.warm = D0 is not None
@@ -575,50 +576,91 @@ class DeviceSCFState:
         dD = self.g._pre(self.it < self.ncyc)
         return dD, self.g.F
 
+    @classmethod
+    def _lane(cls, torch, dev, lane):
+        """Lane ``lane`` of device ``dev``: (graph memory pool, stream).  The
+        post-build graphs of one lane share its pool and replay one after another on
+        its stream, which makes the sharing safe; different lanes' graphs run
+        concurrently.  The pool is owned by a small anchor graph that lives as long
+        as the process (a pool dies with its last graph)."""
+        key = (str(dev), lane)
+        if key not in cls._pools:
+            main = torch.cuda.current_stream(dev)
+            # the stream is this process's own (not one of torch's pool streams,
+            # which other threads can be handed too: their work would land in a
+            # capture)
+            pool = torch.cuda.graph_pool_handle()
+            cs = own_stream(dev.index if dev.index is not None else torch.cuda.current_device())
+            x = torch.zeros(1, device=dev)
+            anchor = torch.cuda.CUDAGraph()
+            cs.wait_stream(main)
+            with torch.cuda.stream(cs):
+                # this thread's cuBLAS handle and the stream's workspace are
+                # created outside any capture
+                w = torch.ones((2, 4, 4), dtype=torch.float64, device=dev)
+                torch.einsum("k,kij->ij", w[:, 0, 0], w) @ w[0]
+                torch.cuda.synchronize(dev)
+                anchor.capture_begin(pool=pool, capture_error_mode="thread_local")
+                y = x + 1.0
+                anchor.capture_end()
+            main.wait_stream(cs)
+            cls._pools[key] = (pool, cs, anchor, x, y)
+        return cls._pools[key][:2]
+
+    def _replay(self):
+        """Capture the post-build half on this solve's lane (first call, or after
+        a recapture is due) and enqueue its replay there.  The caller orders the
+        lane after the Fock build and the next reader after the lane."""
+        torch = self.rhf.torch
+        pool, cs = self._lane(torch, self.rhf.device, self.lane)
+        with torch.cuda.stream(cs):
+            if self.post_graph is None:
+                gr = torch.cuda.CUDAGraph()
+                # thread_local: set-up threads may allocate while this thread captures
+                gr.capture_begin(pool=pool, capture_error_mode="thread_local")
+                self.g._post()
+                gr.capture_end()
+                self.post_graph = gr
+            self.post_graph.replay()
+        return cs
+
     def step_device(self):
         if not self.use_graph:
             self.g._post()
             return self.g.out
         torch = self.rhf.torch
-        dev = self.rhf.device
-        if self.post_graph is None:
-            key = str(dev)
-            main = torch.cuda.current_stream(dev)
-            if key not in DeviceSCFState._pools:
-                # one memory pool for every solve's graph (they replay one after
-                # another on one stream), owned by a small anchor graph that lives
-                # as long as the process: a pool dies with its last graph
-                # the capture stream is this process's own (not one of torch's pool
-                # streams, which other threads can be handed too: their work would
-                # land in the capture); it lives as long as the pool
-                pool = torch.cuda.graph_pool_handle()
-                cs = own_stream(dev.index if dev.index is not None else torch.cuda.current_device())
-                x = torch.zeros(1, device=dev)
-                anchor = torch.cuda.CUDAGraph()
-                cs.wait_stream(main)
-                with torch.cuda.stream(cs):
-                    # this thread's cuBLAS handle and the stream's workspace are
-                    # created outside any capture
-                    w = torch.ones((2, 4, 4), dtype=torch.float64, device=dev)
-                    torch.einsum("k,kij->ij", w[:, 0, 0], w) @ w[0]
-                    torch.cuda.synchronize(dev)
-                    anchor.capture_begin(pool=pool, capture_error_mode="thread_local")
-                    y = x + 1.0
-                    anchor.capture_end()
-                main.wait_stream(cs)
-                DeviceSCFState._pools[key] = (pool, cs, anchor, x, y)
-            pool, cs = DeviceSCFState._pools[key][:2]
-            cs.wait_stream(main)
-            gr = torch.cuda.CUDAGraph()
-            with torch.cuda.stream(cs):
-                # thread_local: set-up threads may allocate while this thread captures
-                gr.capture_begin(pool=pool, capture_error_mode="thread_local")
-                self.g._post()
-                gr.capture_end()
-            main.wait_stream(cs)
-            self.post_graph = gr
-        self.post_graph.replay()
+        main = torch.cuda.current_stream(self.rhf.device)
+        _, cs = self._lane(torch, self.rhf.device, self.lane)
+        cs.wait_stream(main)
+        main.wait_stream(self._replay())
         return self.g.out
+
+    @staticmethod
+    def step_many(states):
+        """``step_device`` of many solves after one (batched) Fock build: every
+        lane waits once for the build, each solve's post-build graph replays on its
+        lane (lanes run concurrently), the current stream waits once per lane.
+        Returns the solves' (Eel, PRMS, PCHANGE, defect) vectors, stacked."""
+        if not states:
+            return None
+        torch = states[0].rhf.torch
+        dev = states[0].rhf.device
+        main = torch.cuda.current_stream(dev)
+        ev = main.record_event()
+        lanes = {}
+        for st in states:
+            if st.use_graph and st.lane not in lanes:
+                _, cs = st._lane(torch, dev, st.lane)
+                cs.wait_event(ev)
+                lanes[st.lane] = cs
+        for st in states:
+            if st.use_graph:
+                st._replay()
+            else:
+                st.g._post()
+        for cs in lanes.values():
+            main.wait_stream(cs)
+        return torch.stack([st.g.out for st in states])
 
     def step(self, vals):
         g, r = self.g, self.rhf

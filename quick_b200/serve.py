@@ -213,7 +213,7 @@ def request_bytes_estimate_mol(mol, name: str, maxdiis: int = 10) -> int:
 
 
 class _Job:
-    __slots__ = ("req", "eng", "rhf", "st", "bytes", "measured", "admitted", "warm")
+    __slots__ = ("req", "eng", "rhf", "st", "bytes", "measured", "admitted", "warm", "lane", "load")
 
 
 class Server:
@@ -232,12 +232,16 @@ class Server:
     ``scf``: "device" advances each solve with :class:`DeviceSCFState` (DIIS on
     the device, SP2 density: no host synchronisation inside a step; the
     post-build half of its cycle captured once as a CUDA graph); "eigh" with
-    :class:`SCFState` (torch eigh, one synchronisation per solve and step)."""
+    :class:`SCFState` (torch eigh, one synchronisation per solve and step).
+    ``lanes``: streams (each with its own graph memory pool) over which the
+    solves' post-build graphs are spread; a solve keeps its lane, and joins the
+    one with the least SP2 work (sum of m^3) at admission.  The post-build half is
+    a chain of small kernels per solve, so solves on different lanes overlap."""
 
     def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
                  denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
                  max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64,
-                 workers: int = 4, scf: str = "device", reserve_sms: int = 0):
+                 workers: int = 4, scf: str = "device", reserve_sms: int = 0, lanes: int = 4):
         import torch
         from .get2e import Get2eBatch
         self.torch = torch
@@ -284,6 +288,8 @@ class Server:
         self.executor = ThreadPoolExecutor(max_workers=workers) if workers > 0 else None
         self._tls = threading.local()
         self._own_streams = []        # the set-up threads' streams, freed by close()
+        self.lanes = max(1, int(lanes))
+        self.lane_load = [0.0] * self.lanes
         self._streams_lock = threading.Lock()
         self.setting_up = []          # (future, request, reserved bytes, admission time)
 
@@ -335,6 +341,11 @@ class Server:
         self.main_stream.wait_event(ev)
         j = _Job()
         j.req, j.eng, j.rhf, j.st = req, eng, rhf, st
+        j.load = float(rhf.X.shape[1]) ** 3
+        j.lane = min(range(self.lanes), key=lambda k: self.lane_load[k])
+        self.lane_load[j.lane] += j.load
+        if hasattr(st, "lane"):
+            st.lane = j.lane
         j.warm = st.warm
         j.admitted = admitted
         j.measured = False
@@ -415,9 +426,13 @@ class Server:
         return list(act)
 
     def _finish(self, act, clock):
+        from .scf import DeviceSCFState
         torch = self.torch
         t1 = time.perf_counter()
-        v = torch.stack([j.st.step_device() for j in act])
+        if self.scf == "device":
+            v = DeviceSCFState.step_many([j.st for j in act])
+        else:
+            v = torch.stack([j.st.step_device() for j in act])
         t2 = time.perf_counter()
         vals = v.cpu().numpy()
         t3 = time.perf_counter()
@@ -445,6 +460,7 @@ class Server:
         if done:
             t = clock()
             for j in done:
+                self.lane_load[j.lane] -= j.load
                 r = j.st.result()
                 req = j.req
                 if req.series is not None:
@@ -581,11 +597,12 @@ def _max_dE(results, ref_E):
 
 
 def run_stream(n_requests: int, rate: float, fp32_bound: float = 0.0, seed: int = 20261203,
-               memory_budget: int = None, denserms: float = 1e-6, device: int = 0, workers: int = 4, **stream_kw):
+               memory_budget: int = None, denserms: float = 1e-6, device: int = 0, workers: int = 4, lanes: int = 4,
+               **stream_kw):
     """Serve one seeded stream; returns (summary dict, results)."""
     reqs = request_stream(n_requests, rate, seed=seed, **stream_kw)
     srv = Server(device=device, memory_budget=memory_budget, fp32_bound=fp32_bound, denserms=denserms,
-                 workers=workers)
+                 workers=workers, lanes=lanes)
     try:
         res = srv.serve(reqs, realtime=True)
         s = summarize(res, srv.wall)
@@ -618,6 +635,7 @@ def main(argv=None):
                     help="serve each stream in plain FP64 and in the mixed form; report |dE| per request")
     ap.add_argument("--budget-gb", type=float, default=None)
     ap.add_argument("--workers", type=int, default=4, help="set-up threads")
+    ap.add_argument("--lanes", type=int, default=4, help="streams the post-build graphs are spread over")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--out", default=None)
     ap.add_argument("--warmup", type=int, default=64,
@@ -628,7 +646,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     budget = int(a.budget_gb * (1 << 30)) if a.budget_gb else None
     if a.warmup > 0:
-        w = Server(memory_budget=budget, workers=a.workers)
+        w = Server(memory_budget=budget, workers=a.workers, lanes=a.lanes)
         w.serve(request_stream(a.warmup, 1000.0, seed=a.seed + 1), realtime=False)
         w.close()
     report = []
@@ -639,9 +657,9 @@ def main(argv=None):
         report.append({"sequential_fp64": seq})
     for rate in a.rate:
         if a.compare:
-            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget, workers=a.workers)
+            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget, workers=a.workers, lanes=a.lanes)
             bound = a.fp32_bound if a.fp32_bound > 0 else 1e-5
-            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget, workers=a.workers)
+            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget, workers=a.workers, lanes=a.lanes)
             e64 = {r.rid: r.E for r in r64}
             dE = [abs(r.E - e64[r.rid]) for r in r32 if r.rid in e64]
             s32["max_abs_dE_vs_fp64"] = float(max(dE)) if dE else None
@@ -654,7 +672,7 @@ def main(argv=None):
                 line["mixed_vs_sequential_fp64"] = s32["solves_per_s"] / seq["solves_per_s"]
                 line["fp64_vs_sequential_fp64"] = s64["solves_per_s"] / seq["solves_per_s"]
         else:
-            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget, workers=a.workers)
+            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget, workers=a.workers, lanes=a.lanes)
             if seq:
                 line["vs_sequential_fp64"] = line["solves_per_s"] / seq["solves_per_s"]
         print(json.dumps(line), flush=True)
