@@ -547,6 +547,61 @@ def measure(name, args, dev, stream, flush, local, world, pg, full):
     return res
 
 
+SERVE_RATE = 200.0
+SERVE_SEED = 20261203
+SERVE_BOUND = 1e-5
+
+
+def serving_figures(args, baselines):
+    """The served form on a short seeded stream (requests of 1-40 waters in STO-3G
+    or 6-31G*, a quarter QM/MM repeats with 4000 point charges, Poisson arrivals at
+    SERVE_RATE): the mixed form served with continuous batching against the plain
+    FP64 path solving the same requests one at a time (``run_sequential``), with
+    |dE| per request against the sequential FP64 energies and, in the baselines
+    leg, against the oracle's SCF on a sample of the requests."""
+    from quick_b200.serve import Server, request_stream, run_sequential, run_stream, _max_dE
+    w = Server(workers=args.serve_workers)
+    w.serve(request_stream(32, 1000.0, seed=SERVE_SEED + 1), realtime=False)
+    w.close()
+    n = args.serve_requests
+    seq, rseq = run_sequential(request_stream(n, 1.0, seed=SERVE_SEED))
+    served, rsrv = run_stream(n, SERVE_RATE, SERVE_BOUND, SERVE_SEED, workers=args.serve_workers,
+                              lanes=args.serve_lanes)
+    e_seq = {r.rid: r.E for r in rseq}
+    out = {"requests": n, "rate_per_s": SERVE_RATE, "fp32_bound": SERVE_BOUND, "workers": args.serve_workers,
+           "lanes": args.serve_lanes,
+           "served_mixed": {k: served[k] for k in ("solves_per_s", "p50_ms", "p99_ms", "mean_iterations", "converged",
+                                                   "mean_batch", "max_batch", "peak_bytes", "molecule", "qmmm")
+                            if k in served},
+           "sequential_fp64": {k: seq[k] for k in ("solves_per_s", "p50_ms", "p99_ms", "mean_iterations", "converged")},
+           "served_over_sequential": served["solves_per_s"] / seq["solves_per_s"],
+           "max_abs_dE_served_mixed_vs_sequential_fp64": _max_dE(rsrv, e_seq),
+           "stream": "seeded: Poisson arrivals; 1-40 waters log-uniform, basis uniform over {STO-3G, 6-31G*}; "
+                     "25% QM/MM repeats (20-water QM region, 4000 TIP3P point charges, warm start)"}
+    if baselines:
+        # the oracle's RHF (same cutoffs, tight convergence) on a sample of the requests:
+        # the smallest molecule requests of each basis and the first QM/MM request
+        from oracle import oracle as O
+        from quick_b200.basis import build_basis
+        reqs = {r.rid: r for r in request_stream(n, 1.0, seed=SERVE_SEED)}
+        got = {r.rid: r for r in rsrv}
+        mols = sorted((r for r in reqs.values() if r.kind == "molecule"), key=lambda r: (len(r.mol.Z), r.rid))
+        pick = [r for b in ("STO-3G", "6-31G*") for r in [x for x in mols if x.basis == b][:2]]
+        pick += [r for r in reqs.values() if r.kind == "qmmm"][:1]
+        rows = []
+        t0 = time.perf_counter()
+        for r in pick:
+            b = build_basis(r.mol, r.basis)
+            ref = O.rhf(b, integral_cutoff=1e-10, prim_limit=1e-11, conv=1e-8, ext_charges=r.ext_charges)
+            rows.append({"rid": r.rid, "kind": r.kind, "basis": r.basis, "nbasis": b.nbasis,
+                         "abs_dE_served_mixed_vs_oracle": abs(got[r.rid].E - ref["E"]),
+                         "abs_dE_sequential_fp64_vs_oracle": abs(e_seq[r.rid] - ref["E"])})
+        out["vs_oracle"] = {"sample": rows, "max_abs_dE_served_mixed": max(x["abs_dE_served_mixed_vs_oracle"]
+                                                                          for x in rows),
+                            "oracle_seconds": round(time.perf_counter() - t0, 1)}
+    return out
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -568,6 +623,11 @@ def run_ours(args):
     if not args.no_extra:
         for wl in [w for w in EXTRA_WORKLOADS if w != args.workload]:
             extras[wl] = measure(wl, args, dev, stream, flush, local, world, pg, full=False)
+    serving = None
+    if not args.no_serve and world == 1:
+        del flush
+        torch.cuda.empty_cache()
+        serving = serving_figures(args, baselines=not args.no_cpu)
 
     if rank == 0:
         line = {
@@ -581,7 +641,7 @@ def run_ours(args):
             "reference_gpu": head.get("reference_gpu"), "parity_vs_oracle": head.get("parity_vs_oracle"),
             "scf": head.get("scf"), "mixed": head.get("mixed"),
             "bit_identical_host_vs_device": head["bit_identical_host_vs_device"], "classes": head["classes"],
-            "autotune": head.get("autotune"),
+            "autotune": head.get("autotune"), "serving": serving,
             "workloads": {k: {kk: v[kk] for kk in ("workload", "nbasis", "value", "ms_per_step", "e2e", "scf", "mixed",
                                                    "roofline", "launches_per_build") if kk in v}
                           for k, v in extras.items()},
@@ -619,6 +679,10 @@ def main():
                     help="skip the baselines leg (CPU oracle sample, QUICK's GPU get2e, parity vs the oracle)")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg (1 GPU only)")
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-workers", type=int, default=8)
+    ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -311,6 +311,15 @@ int qk_small_solve(const double *A_dev, const double *b_dev, int n, double *x_de
  * 155115 (2002)).  Yout must not alias Y or Y2.  The traces and the update are one
  * launch, so a captured SCF iteration holds two nodes per step (the GEMM and this). */
 int qk_sp2_step(const double *Y_dev, const double *Y2_dev, double *Yout_dev, int n, double nocc, void *stream);
+/* `steps` SP2 steps on `stream`, each the GEMM Y2 = Y Y (cuBLAS DGEMM) and
+ * qk_sp2_step, with Ya and Yb as ping-pong buffers: the purified matrix ends in Ya
+ * when `steps` is even, in Yb when it is odd.  One call instead of 2 x steps, so that
+ * a host loop -- or the capture of one into a CUDA graph -- costs one call whatever
+ * the step count.  The first call on a device creates the library's cuBLAS handle
+ * for that device (steps = 0 does only that): it must come before any stream
+ * capture; inside a capture it returns QK_ERR_NOT_READY instead.  The handle runs
+ * without a workspace, so calls on different streams share no scratch memory. */
+int qk_sp2_run(double *Ya_dev, double *Yb_dev, double *Y2_dev, int n, double nocc, int steps, void *stream);
 
 /* One-electron integrals on device `device` (replaces the get1e path and the
  * reference's gpu_get_oei_, src/gpu/gpu_oei.cu:194; CPU twin

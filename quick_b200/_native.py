@@ -26,7 +26,7 @@ EXPORTED = [
     "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_sp2_step", "qk_set_shard", "qk_fock2e_device_accumulate", "qk_finalize_fixed", "qk_set_streams",
     "qk_set_class_launch", "qk_class_launch", "qk_batch_reserve_sms", "qk_boys", "qk_set_boys", "qk_set_worklist_builder",
     "gpu_upload_calculated_beta_", "gpu_get_oshell_eri_", "qk_fock2e_uhf_device", "qk_fock2e_uhf_host",
-    "qk_stream_create", "qk_stream_destroy",
+    "qk_stream_create", "qk_stream_destroy", "qk_sp2_run",
 ]
 
 _lib = None
@@ -95,6 +95,7 @@ def lib():
     L.qk_class_launch.argtypes = [P, I, PI, PI, PI, PI]
     L.qk_small_solve.argtypes = [P, P, I, P, P, P]
     L.qk_sp2_step.argtypes = [P, P, P, I, ctypes.c_double, P]
+    L.qk_sp2_run.argtypes = [P, P, P, I, ctypes.c_double, I, P]
     L.qk_set_shard.argtypes = [P, I, I]
     L.qk_fock2e_device_accumulate.argtypes = [P, P, P, P, P]
     L.qk_finalize_fixed.argtypes = [P, I, P, P]

@@ -15,7 +15,10 @@ MAX_L = 3
 # --split-compile=0: the device optimiser runs over the kernels in parallel on all
 # host cores (the class kernels are independent; the build takes half the time)
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", f"-DQK_MAX_L={MAX_L}", "--split-compile=0"]
+              "-Xcompiler", "-fPIC", "-shared", f"-DQK_MAX_L={MAX_L}", "--split-compile=0",
+              # cuBLAS for the SP2 GEMMs of the SCF driver (scf.cu); in a process that
+              # has loaded torch, its libcublas.so.12 serves this dependency
+              "-lcublas", "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
 
 
 def sources():

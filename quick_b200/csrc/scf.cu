@@ -6,10 +6,13 @@
 // LAPACK) -- at most 64 unknowns -- by Gaussian elimination with partial
 // pivoting in one warp, the matrix held in shared memory.  A zero or non-finite
 // pivot sets *ok = 0 (the caller then keeps the plain Fock matrix).
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 
 #include "quick_b200.h"
 
@@ -117,7 +120,67 @@ __global__ void __launch_bounds__(kSp2Threads) sp2_step_kernel(const double* __r
         Yout[k] = sq ? Y2[k] : 2.0 * Y[k] - Y2[k];
 }
 
+// The GEMM of the SP2 steps is cuBLAS's DGEMM, one handle per device, shared by every
+// stream (the enqueue is serialised by a mutex).  The handle runs without a workspace,
+// so that calls on different streams share no scratch memory and a call inside a
+// stream capture allocates nothing; it is created by the first call on the device,
+// which must come before any capture.
+struct BlasHandles {
+    std::mutex mu;
+    std::map<int, cublasHandle_t> by_device;
+};
+
+static BlasHandles& blas_handles() {
+    static BlasHandles b;
+    return b;
+}
+
+// The current device's handle, bound to `s` with no workspace.  Caller holds the mutex.
+static int blas_on(cudaStream_t s, cublasHandle_t* out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return QK_ERR_CUDA;
+    auto& m = blas_handles().by_device;
+    auto it = m.find(dev);
+    if (it == m.end()) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (s && cudaStreamIsCapturing(s, &cap) != cudaSuccess) return QK_ERR_CUDA;
+        if (cap != cudaStreamCaptureStatusNone) return QK_ERR_NOT_READY;   // creating it would allocate
+        cublasHandle_t h = nullptr;
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return QK_ERR_CUDA;
+        it = m.emplace(dev, h).first;
+    }
+    if (cublasSetStream(it->second, s) != CUBLAS_STATUS_SUCCESS ||
+        cublasSetWorkspace(it->second, nullptr, 0) != CUBLAS_STATUS_SUCCESS)
+        return QK_ERR_CUDA;
+    *out = it->second;
+    return QK_OK;
+}
+
 }  // namespace qk
+
+extern "C" int qk_sp2_run(double* Ya, double* Yb, double* Y2, int n, double nocc, int steps, void* stream) {
+    if (!Ya || !Yb || !Y2 || n < 1 || steps < 0 || Ya == Yb || Ya == Y2 || Yb == Y2) return QK_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nn = (size_t)n * n;
+    const int grid = (int)std::min<size_t>(4 * 148, (nn + qk::kSp2Threads - 1) / qk::kSp2Threads);
+    std::lock_guard<std::mutex> guard(qk::blas_handles().mu);
+    cublasHandle_t h = nullptr;
+    const int st = qk::blas_on(s, &h);
+    if (st != QK_OK) return st;
+    const double one = 1.0, zero = 0.0;
+    double* cur = Ya;
+    double* nxt = Yb;
+    for (int k = 0; k < steps; ++k) {
+        // row-major Y2 = Y Y is column-major Y2^T = Y^T Y^T: the same call
+        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, cur, n, cur, n, &zero, Y2, n) !=
+            CUBLAS_STATUS_SUCCESS)
+            return QK_ERR_CUDA;
+        qk::sp2_step_kernel<<<grid, qk::kSp2Threads, 0, s>>>(cur, Y2, nxt, n, nocc);
+        if (cudaGetLastError() != cudaSuccess) return QK_ERR_CUDA;
+        std::swap(cur, nxt);
+    }
+    return QK_OK;
+}
 
 extern "C" int qk_sp2_step(const double* Y, const double* Y2, double* Yout, int n, double nocc, void* stream) {
     if (!Y || !Y2 || !Yout || n < 1 || Yout == Y || Yout == Y2) return QK_ERR_INVALID_ARG;

@@ -379,6 +379,11 @@ class GraphSCF:
         self.eye_k = torch.eye(k, dtype=dt, device=dev)
         self.eye_m = torch.eye(m, dtype=dt, device=dev)
         self.Ya, self.Yb, self.Y2 = z(m, m), z(m, m), z(m, m)   # SP2 iterates (ping-pong) and Y Y
+        # zero steps: creates the library's cuBLAS handle for the device now, outside
+        # any graph capture (creating it inside one would allocate)
+        check(lib().qk_sp2_run(ctypes.c_void_p(self.Ya.data_ptr()), ctypes.c_void_p(self.Yb.data_ptr()),
+                               ctypes.c_void_p(self.Y2.data_ptr()), m, 0.0, 0,
+                               ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)), "qk_sp2_run")
         self.out = z(4)
         self.cycle = torch.zeros((), dtype=torch.int64, device=dev)
         self.XtS = rhf.X.T @ rhf.S          # orthogonal-basis projector of D: (XtS) D (XtS)^T / 2
@@ -403,17 +408,14 @@ class GraphSCF:
         rad = torch.abs(Fo).sum(dim=1) - torch.abs(d)
         emin, emax = torch.min(d - rad), torch.max(d + rad)
         ne = float(self.rhf.nocc)
-        cur, nxt = self.Ya, self.Yb
-        torch.div(emax * self.eye_m - Fo, emax - emin, out=cur)
-        # each step: one GEMM and one fused trace-test-and-update launch
+        torch.div(emax * self.eye_m - Fo, emax - emin, out=self.Ya)
+        # all steps in one call (each: the symmetric square and one fused
+        # trace-test-and-update launch); the result is in Ya after an even count
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.rhf.device).cuda_stream)
-        m = cur.shape[0]
-        for _ in range(self.sp2):
-            torch.mm(cur, cur, out=self.Y2)
-            check(lib().qk_sp2_step(ctypes.c_void_p(cur.data_ptr()), ctypes.c_void_p(self.Y2.data_ptr()),
-                                    ctypes.c_void_p(nxt.data_ptr()), m, ne, stream), "qk_sp2_step")
-            cur, nxt = nxt, cur
-        Y = cur
+        m = self.Ya.shape[0]
+        check(lib().qk_sp2_run(ctypes.c_void_p(self.Ya.data_ptr()), ctypes.c_void_p(self.Yb.data_ptr()),
+                               ctypes.c_void_p(self.Y2.data_ptr()), m, ne, self.sp2, stream), "qk_sp2_run")
+        Y = self.Ya if self.sp2 % 2 == 0 else self.Yb
         # idempotency defect tr(Y - Y^2): zero once the projection has converged
         self.out[3].copy_(torch.trace(Y) - torch.sum(Y * Y))
         return 2.0 * (X @ Y @ X.T)
@@ -649,7 +651,7 @@ class DeviceSCFState:
         ev = main.record_event()
         lanes = {}
         for st in states:
-            if st.use_graph and st.lane not in lanes:
+            if st.lane not in lanes:
                 _, cs = st._lane(torch, dev, st.lane)
                 cs.wait_event(ev)
                 lanes[st.lane] = cs
@@ -657,7 +659,8 @@ class DeviceSCFState:
             if st.use_graph:
                 st._replay()
             else:
-                st.g._post()
+                with torch.cuda.stream(lanes[st.lane]):
+                    st.g._post()
         for cs in lanes.values():
             main.wait_stream(cs)
         return torch.stack([st.g.out for st in states])

@@ -241,7 +241,8 @@ class Server:
     def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
                  denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
                  max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64,
-                 workers: int = 4, scf: str = "device", reserve_sms: int = 0, lanes: int = 4):
+                 workers: int = 4, scf: str = "device", reserve_sms: int = 0, lanes: int = 4,
+                 post_graph: bool = True):
         import torch
         from .get2e import Get2eBatch
         self.torch = torch
@@ -289,6 +290,7 @@ class Server:
         self._tls = threading.local()
         self._own_streams = []        # the set-up threads' streams, freed by close()
         self.lanes = max(1, int(lanes))
+        self.post_graph = post_graph
         self.lane_load = [0.0] * self.lanes
         self._streams_lock = threading.Lock()
         self.setting_up = []          # (future, request, reserved bytes, admission time)
@@ -327,7 +329,7 @@ class Server:
             rhf = RHF(basis, device=self.device, ext_charges=req.ext_charges, engine=eng)
             if self.scf == "device":
                 st = DeviceSCFState(rhf, denserms=self.denserms, maxiter=self.maxiter, D0=D0, maxdiis=self.maxdiis,
-                                    graph=True)
+                                    graph=self.post_graph)
             else:
                 st = rhf.state(denserms=self.denserms, maxiter=self.maxiter, maxdiis=self.maxdiis, D0=D0)
             ev = torch.cuda.Event()

@@ -78,6 +78,46 @@ def test_sp2_step_matches_formula(n, nocc):
     assert lib().qk_sp2_step(vp(Y), vp(Y2), vp(Y), n, nocc, ctypes.c_void_p(s.cuda_stream)) != 0   # aliasing refused
 
 
+@pytest.mark.parametrize("n,nocc,steps", [(37, 5.0, 0), (37, 5.0, 7), (37, 5.0, None), (300, 41.0, None),
+                                           (608, 160.0, None)])
+def test_sp2_run_equals_stepwise_loop(n, nocc, steps):
+    """qk_sp2_run against the same steps taken one at a time from Python (torch's
+    GEMM and qk_sp2_step): the same matrix to 1e-12 (both GEMMs are cuBLAS's, run
+    through different handles), result in Ya after an even step count and Yb after
+    an odd one; with the SCF's step count (sp2_steps) the purified matrix is
+    idempotent with trace nocc."""
+    _cuda()
+    from quick_b200._native import check, lib
+    from quick_b200.scf import sp2_steps
+    g = torch.Generator().manual_seed(n)
+    A = torch.randn(n, n, generator=g, dtype=torch.float64)
+    _, U = torch.linalg.eigh((A + A.T) / 2.0)
+    w = torch.linspace(-2.0, 1.0, n, dtype=torch.float64)          # a clean gap at every nocc
+    F = (U * w) @ U.T
+    d = torch.diagonal(F)
+    rad = F.abs().sum(dim=1) - d.abs()
+    emin, emax = float((d - rad).min()), float((d + rad).max())
+    Y0 = ((emax * torch.eye(n, dtype=torch.float64) - F) / (emax - emin)).cuda()
+    converge = steps is None
+    if converge:
+        steps = sp2_steps(w.numpy(), int(nocc), emax - emin)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    Ya, Yb, Y2 = Y0.clone(), torch.zeros_like(Y0), torch.zeros_like(Y0)
+    check(lib().qk_sp2_run(vp(Ya), vp(Yb), vp(Y2), n, nocc, steps, s), "qk_sp2_run")
+    got = Ya if steps % 2 == 0 else Yb
+    cur, nxt, Z2 = Y0.clone(), torch.zeros_like(Y0), torch.zeros_like(Y0)
+    for _ in range(steps):
+        torch.mm(cur, cur, out=Z2)
+        check(lib().qk_sp2_step(vp(cur), vp(Z2), vp(nxt), n, nocc, s), "qk_sp2_step")
+        cur, nxt = nxt, cur
+    assert float((got - cur).abs().max()) <= 1e-12
+    if converge:
+        assert abs(float(torch.trace(got)) - nocc) < 1e-8
+        assert float((got @ got - got).abs().max()) < 1e-8
+    assert lib().qk_sp2_run(vp(Ya), vp(Ya), vp(Y2), n, nocc, steps, s) != 0   # aliasing refused
+
+
 def test_sp2_projector_equals_diagonalisation():
     _cuda()
     from quick_b200.scf import RHF, GraphSCF, gershgorin_range, sp2_steps
