@@ -119,19 +119,39 @@ def check(status: int, what: str = "quick_b200"):
         raise QuickError(status, what)
 
 
+_free_streams = {}          # (device, high_priority) -> streams given back by free_stream
+_streams_lock = None
+
+
 def own_stream(device: int, high_priority: bool = True):
     """A torch view of a stream created for the caller alone (qk_stream_create).
 
     torch's ``torch.cuda.Stream`` hands out streams from a fixed pool per priority,
     round robin, so two threads can be given the same stream; a thread that captures
     a CUDA graph on a shared stream has its capture invalidated (or other work
-    captured into it) when another thread enqueues there.  Free the stream with
-    :func:`free_stream` after its work is done."""
+    captured into it) when another thread enqueues there.  Give the stream back with
+    :func:`free_stream` once its work is done: it is kept for the next caller, not
+    destroyed, since torch's allocators keep per-stream state for as long as the
+    process runs."""
+    global _streams_lock
+    import threading
     import torch
+    if _streams_lock is None:
+        _streams_lock = threading.Lock()
+    key = (int(device), bool(high_priority))
+    with _streams_lock:
+        free = _free_streams.get(key)
+        if free:
+            return free.pop()
     p = ctypes.c_void_p()
     check(lib().qk_stream_create(int(device), 1 if high_priority else 0, ctypes.byref(p)), "qk_stream_create")
-    return torch.cuda.ExternalStream(p.value, device=torch.device("cuda", int(device)))
+    s = torch.cuda.ExternalStream(p.value, device=torch.device("cuda", int(device)))
+    s._qk_key = key
+    return s
 
 
 def free_stream(stream) -> None:
-    check(lib().qk_stream_destroy(ctypes.c_void_p(stream.cuda_stream)), "qk_stream_destroy")
+    """Give a stream from :func:`own_stream` back for reuse (its queued work
+    must be finished or ordered before the next owner's)."""
+    with _streams_lock:
+        _free_streams.setdefault(stream._qk_key, []).append(stream)

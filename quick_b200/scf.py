@@ -638,16 +638,18 @@ class DeviceSCFState:
         return self.g.out
 
     @staticmethod
-    def step_many(states):
+    def step_many(states, join=None):
         """``step_device`` of many solves after one (batched) Fock build: every
         lane waits once for the build, each solve's post-build graph replays on its
-        lane (lanes run concurrently), the current stream waits once per lane.
-        Returns the solves' (Eel, PRMS, PCHANGE, defect) vectors, stacked."""
+        lane (lanes run concurrently), then ``join`` (default: the current stream)
+        waits once per lane.  Returns the solves' (Eel, PRMS, PCHANGE, defect)
+        vectors, stacked on ``join``."""
         if not states:
             return None
         torch = states[0].rhf.torch
         dev = states[0].rhf.device
         main = torch.cuda.current_stream(dev)
+        join = main if join is None else join
         ev = main.record_event()
         lanes = {}
         for st in states:
@@ -662,8 +664,9 @@ class DeviceSCFState:
                 with torch.cuda.stream(lanes[st.lane]):
                     st.g._post()
         for cs in lanes.values():
-            main.wait_stream(cs)
-        return torch.stack([st.g.out for st in states])
+            join.wait_stream(cs)
+        with torch.cuda.stream(join):
+            return torch.stack([st.g.out for st in states])
 
     def step(self, vals):
         g, r = self.g, self.rhf

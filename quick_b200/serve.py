@@ -213,7 +213,7 @@ def request_bytes_estimate_mol(mol, name: str, maxdiis: int = 10) -> int:
 
 
 class _Job:
-    __slots__ = ("req", "eng", "rhf", "st", "bytes", "measured", "admitted", "warm", "lane", "load")
+    __slots__ = ("req", "eng", "rhf", "st", "bytes", "measured", "admitted", "warm", "lane", "load", "cohort")
 
 
 class Server:
@@ -236,13 +236,20 @@ class Server:
     ``lanes``: streams (each with its own graph memory pool) over which the
     solves' post-build graphs are spread; a solve keeps its lane, and joins the
     one with the least SP2 work (sum of m^3) at admission.  The post-build half is
-    a chain of small kernels per solve, so solves on different lanes overlap."""
+    a chain of small kernels per solve, so solves on different lanes overlap.
+    ``post_graph``: capture each solve's post-build half as a CUDA graph (else it
+    runs eagerly on its lane).
+    ``pipeline``: split the solves into two cohorts stepped in turn, so that one
+    cohort's post-build halves and read-back run while the other's Fock build
+    runs, and the host takes one cohort's figures while the GPU works on the other;
+    ``reserve_sms`` then leaves that many SMs to the post-build kernels while a
+    batch's persistent Fock kernels run."""
 
     def __init__(self, device: int = 0, memory_budget: int = None, fp32_bound: float = 0.0,
                  denserms: float = 1e-6, maxiter: int = 100, integral_cutoff: float = 1e-10,
                  max_active: int = 512, maxdiis: int = 10, keep_densities: bool = False, pool: int = 64,
                  workers: int = 4, scf: str = "device", reserve_sms: int = 0, lanes: int = 4,
-                 post_graph: bool = True):
+                 post_graph: bool = True, pipeline: bool = True):
         import torch
         from .get2e import Get2eBatch
         self.torch = torch
@@ -272,6 +279,7 @@ class Server:
         self.peak_used = 0
         self.steps = 0
         self.batch_sizes = []
+        self.max_concurrent = 0       # most solves in flight at once
         self.rejected = []
         self.timers = {"admit": 0.0, "setup_engine": 0.0, "setup_rhf": 0.0, "fock": 0.0, "scf": 0.0, "sync": 0.0,
                        "retire": 0.0, "fock_gpu": 0.0}
@@ -288,9 +296,24 @@ class Server:
         (a @ a).sum().item()
         self.executor = ThreadPoolExecutor(max_workers=workers) if workers > 0 else None
         self._tls = threading.local()
-        self._own_streams = []        # the set-up threads' streams, freed by close()
+        self._own_streams = []        # streams this server took (set-up threads, read-back), given back by close()
         self.lanes = max(1, int(lanes))
         self.post_graph = post_graph
+        # two cohorts stepped in turn (device SCF only): one's post-build halves and
+        # read-back run while the other's Fock build runs.  Each has its own batch
+        # (a batch's staging block serves one build in flight), read-back stream and
+        # pinned buffer of convergence figures.
+        self.pipeline = bool(pipeline) and scf == "device"
+        self.cohorts = [[], []]
+        self.cohort_load = [0.0, 0.0]
+        self._inflight = [None, None]
+        if self.pipeline:
+            self.batches = [self.batch, Get2eBatch(device)]
+            self.batches[1].reserve_sms(reserve_sms)
+            self._rb = [own_stream(device), own_stream(device)]
+            self._own_streams.extend(self._rb)
+            self._pinned = [torch.zeros((max_active, 4), dtype=torch.float64).pin_memory() for _ in range(2)]
+            self._step_done = [None, None]
         self.lane_load = [0.0] * self.lanes
         self._streams_lock = threading.Lock()
         self.setting_up = []          # (future, request, reserved bytes, admission time)
@@ -325,7 +348,10 @@ class Server:
             eng.bind(basis)
         eng.prepare()
         t1 = time.perf_counter()
+        D0, D0_ready = D0 if isinstance(D0, tuple) else (D0, None)
         with torch.cuda.stream(stream):
+            if D0_ready is not None:
+                stream.wait_event(D0_ready)
             rhf = RHF(basis, device=self.device, ext_charges=req.ext_charges, engine=eng)
             if self.scf == "device":
                 st = DeviceSCFState(rhf, denserms=self.denserms, maxiter=self.maxiter, D0=D0, maxdiis=self.maxdiis,
@@ -348,6 +374,10 @@ class Server:
         self.lane_load[j.lane] += j.load
         if hasattr(st, "lane"):
             st.lane = j.lane
+        if self.pipeline:
+            j.cohort = 0 if self.cohort_load[0] <= self.cohort_load[1] else 1
+            self.cohort_load[j.cohort] += j.load
+            self.cohorts[j.cohort].append(j)
         j.warm = st.warm
         j.admitted = admitted
         j.measured = False
@@ -441,10 +471,18 @@ class Server:
         self.timers["scf"] += t2 - t1
         self.timers["sync"] += t3 - t2
         self.timers["fock_gpu"] += self._ev[0].elapsed_time(self._ev[1]) * 1e-3
+        return self._absorb(act, vals, clock, self.main_stream)
+
+    def _absorb(self, act, vals, clock, stream):
+        """Every solve of a finished step takes its convergence figures; the
+        converged ones retire (their density copies are made on ``stream``, on
+        which the step's work is already complete or ordered)."""
+        torch = self.torch
+        t3 = time.perf_counter()
         self.steps += 1
         self.batch_sizes.append(len(act))
+        self.max_concurrent = max(self.max_concurrent, len(self.active))
         done = []
-        ids = {id(j) for j in act}
         for j, v in zip(act, vals):
             if not j.measured:
                 tot, _ = j.eng.device_bytes()
@@ -458,17 +496,29 @@ class Server:
         self.peak_used = max(self.peak_used, self.used)
         gone = {id(j) for j in done}
         self.active = [j for j in self.active if id(j) not in gone]
+        if self.pipeline and gone:
+            self.cohorts = [[j for j in c if id(j) not in gone] for c in self.cohorts]
         out = []
         if done:
             t = clock()
-            for j in done:
+            with torch.cuda.stream(stream):
+                rs = [j.st.result() for j in done]
+                ev = torch.cuda.Event()
+                ev.record(stream)
+            # the copies read the solves' own buffers, which are freed (and may be
+            # handed to a set-up thread's stream) as soon as the solves are dropped
+            ev.synchronize()
+            for j, r in zip(done, rs):
                 self.lane_load[j.lane] -= j.load
-                r = j.st.result()
+                if self.pipeline:
+                    self.cohort_load[j.cohort] -= j.load
                 req = j.req
                 if req.series is not None:
                     self.series_busy.discard(req.series)
                     if r["converged"]:
-                        self.series_D[req.series] = r["D"]
+                        # the next request of the series starts from this density once
+                        # its copy (ordered by ev) is done
+                        self.series_D[req.series] = (r["D"], ev)
                 out.append(Result(req.rid, r["E"], r["niter"], r["converged"], j.rhf.basis.nbasis, req.basis,
                                   req.kind, self._arrival(req), j.admitted, t, j.bytes, j.warm,
                                   r["D"] if self.keep_densities else None))
@@ -482,6 +532,47 @@ class Server:
         self.timers["retire"] += time.perf_counter() - t3
         return out
 
+    # -- the pipelined step (two cohorts)
+    def _launch_cohort(self, k):
+        """Enqueue one step of cohort k: its batched Fock build on the main stream
+        (ordered after the cohort's previous post-build halves), the post-build
+        halves on the lanes, and the read-back of the convergence figures into
+        pinned memory on the cohort's read-back stream."""
+        from .scf import DeviceSCFState
+        torch = self.torch
+        act = list(self.cohorts[k])
+        t0 = time.perf_counter()
+        main = self.main_stream
+        if self._step_done[k] is not None:
+            main.wait_event(self._step_done[k])
+        ins = [j.st.fock_input() for j in act]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        self.batches[k].fock2e([j.eng for j in act], [d for d, _ in ins], os=[f for _, f in ins], stream=main)
+        e1.record(main)
+        t1 = time.perf_counter()
+        rb = self._rb[k]
+        v = DeviceSCFState.step_many([j.st for j in act], join=rb)
+        host = self._pinned[k][: len(act)]
+        with torch.cuda.stream(rb):
+            host.copy_(v, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(rb)
+        self._step_done[k] = done
+        self.timers["fock"] += t1 - t0
+        self.timers["scf"] += time.perf_counter() - t1
+        return act, done, host, v, e0, e1
+
+    def _finish_cohort(self, k, clock):
+        act, done, host, v, e0, e1 = self._inflight[k]
+        self._inflight[k] = None
+        t = time.perf_counter()
+        done.synchronize()
+        vals = host.numpy().copy()
+        self.timers["sync"] += time.perf_counter() - t
+        self.timers["fock_gpu"] += e0.elapsed_time(e1) * 1e-3
+        return self._absorb(act, vals, clock, self._rb[k])
+
     def serve(self, requests, realtime: bool = True):
         """Run a request stream to completion; returns the results in request order.
 
@@ -494,6 +585,29 @@ class Server:
         clock = lambda: time.perf_counter() - t0  # noqa: E731
         self._arrival = arrival
         results = []
+        if self.pipeline:
+            k = 0
+            while pending or self.queue or self.active or self.setting_up or any(self._inflight):
+                now = clock()
+                while pending and arrival(pending[0]) <= now:
+                    self.queue.append(pending.popleft())
+                # cohort k: take its last step's figures (its post-build ran beside the
+                # other cohort's Fock build), then launch its next step
+                if self._inflight[k] is not None:
+                    results.extend(self._finish_cohort(k, clock))
+                self._admit(now)
+                self._collect()
+                if self.cohorts[k]:
+                    self._inflight[k] = self._launch_cohort(k)
+                if not any(self._inflight) and not self.active:
+                    nxt = (arrival(pending[0]) - clock()) if pending else None
+                    if self.setting_up:
+                        self._collect(block_until=nxt if nxt is not None else 60.0)
+                    elif nxt is not None and not self.queue:
+                        time.sleep(max(0.0, nxt))
+                k ^= 1
+            self.wall = clock()
+            return sorted(results, key=lambda r: r.rid)
         while pending or self.queue or self.active or self.setting_up:
             now = clock()
             while pending and arrival(pending[0]) <= now:
@@ -514,6 +628,7 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
     def close(self):
+        self.torch.cuda.synchronize(self.device)
         if self.executor is not None:
             self.executor.shutdown(wait=True)
             for f, _, _, _ in self.setting_up:
@@ -527,7 +642,11 @@ class Server:
         self.active = []
         self.pool = []
         self.used = 0
+        self.cohorts = [[], []]
+        self._inflight = [None, None]
         self.batch.close()
+        if self.pipeline:
+            self.batches[1].close()
         if self._own_streams:
             self.torch.cuda.synchronize(self.device)
             for st in self._own_streams:

@@ -38,7 +38,7 @@ def test_alone_equals_in_mix():
     reqs = _mix()
     srv = Server(keep_densities=True, workers=0)
     mixed = srv.serve(reqs, realtime=False)
-    assert max(srv.batch_sizes) == len(reqs)        # all were in one batch at the start
+    assert srv.max_concurrent == len(reqs)          # all were in flight together at the start
     srv.close()
     for r in reqs:
         s1 = Server(keep_densities=True)
@@ -86,7 +86,7 @@ def test_memory_budget_admission():
     srv = Server(memory_budget=budget)
     res = srv.serve(reqs, realtime=False)
     assert len(res) == len(reqs) and all(r.converged for r in res)
-    assert max(srv.batch_sizes) < len(reqs)
+    assert srv.max_concurrent < len(reqs)
     assert not srv.active and srv.used == sum(b for _, b in srv.pool)
     assert srv.peak_used <= srv.budget
     for a, b in zip(alone, res):
