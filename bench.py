@@ -542,7 +542,7 @@ def measure(name, args, dev, stream, flush, local, world, pg, full):
     if tune_report is not None:
         res["autotune"] = {"ms_default": round(tune_report["ms_default"], 4),
                            "ms_tuned": round(tune_report["ms_tuned"], 4),
-                           "best_streams": tune_report["best_streams"]}
+                           "best_streams": tune_report["best_streams"], "merge_sp": tune_report["merge_sp"]}
     eng.close()
     return res
 

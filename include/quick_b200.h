@@ -254,6 +254,16 @@ int qk_launches_per_build(qk_ctx *ctx);
  * (gpu_upload_cutoff_matrix_, src/gpu/cuda/gpu.cu:879-1470). */
 int qk_set_worklist_builder(qk_ctx *ctx, int on_device);
 
+/* The six per-lane s/p classes (ssss, psss, psps, ppss, ppps, pppp) as one
+ * persistent kernel per precision over their joined work lists, heaviest class
+ * first (on = 1), instead of one launch per class (0, the default).  The Fock
+ * matrix is the same bit for bit; the merged kernel runs every class at the
+ * register allocation of the largest.  The reference walks all classes in one
+ * kernel over the pair-list product (src/gpu/gpu_get2e_subs.h:771).  Applies to
+ * qk_fock2e_device and the calls built on it, not to the allocation-free build,
+ * the many-molecule batch or builds with per-class profiling on. */
+int qk_set_merge_sp(qk_ctx *ctx, int on);
+
 /* A stream of the caller's own: non-blocking, at the device's highest priority
  * (high_priority != 0) or its lowest, owned by nobody else.  Streams handed out by a
  * framework's pool may be shared with other threads; a thread that captures a CUDA

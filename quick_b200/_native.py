@@ -26,7 +26,7 @@ EXPORTED = [
     "qk_device_bytes", "qk_prepare", "qk_small_solve", "qk_sp2_step", "qk_set_shard", "qk_fock2e_device_accumulate", "qk_finalize_fixed", "qk_set_streams",
     "qk_set_class_launch", "qk_class_launch", "qk_batch_reserve_sms", "qk_boys", "qk_set_boys", "qk_set_worklist_builder",
     "gpu_upload_calculated_beta_", "gpu_get_oshell_eri_", "qk_fock2e_uhf_device", "qk_fock2e_uhf_host",
-    "qk_stream_create", "qk_stream_destroy", "qk_sp2_run",
+    "qk_stream_create", "qk_stream_destroy", "qk_sp2_run", "qk_set_merge_sp",
 ]
 
 _lib = None
@@ -65,6 +65,7 @@ def lib():
     L.qk_boys.argtypes = [P, I, P, I, P, P]
     L.qk_set_boys.argtypes = [P, I]
     L.qk_set_worklist_builder.argtypes = [P, I]
+    L.qk_set_merge_sp.argtypes = [P, I]
     L.qk_stream_create.argtypes = [I, I, ctypes.POINTER(ctypes.c_void_p)]
     L.qk_stream_destroy.argtypes = [P]
     L.qk_fock2e_uhf_device.argtypes = [P, P, P, P, P, P, P]

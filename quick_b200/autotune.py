@@ -12,7 +12,11 @@ caller's molecule and density, with CUDA events:
    builds (``qk_set_profiling`` events), and each class keeps its fastest shape;
 2. the stream count (``qk_set_streams``): class kernels concurrent over 1, 2 or 4
    streams, or one after another -- whole builds timed;
-3. optionally (:func:`tune_precision`) the mixed form's Schwarz switch bound:
+3. the s/p classes as one merged kernel (``qk_set_merge_sp``) or one launch per
+   class, with each stream count -- whole builds timed (the merged launch pays on
+   small molecules, whose builds are launch-bound, and loses on large ones, where
+   it runs every s/p class at the largest one's register allocation);
+4. optionally (:func:`tune_precision`) the mixed form's Schwarz switch bound:
    the fastest bound whose SCF energy stays within ``tol`` of plain FP64.
 
 The reference has no counterpart (its kernels are launched with fixed shapes,
@@ -115,13 +119,18 @@ def tune(eng, D, warps=(1, 2, 4, 8), streams=(0, 1, 2, 4), reps: int = 3):
         else:
             set_shape(eng, i, 0)
     st = {}
-    for s in streams:
-        eng.set_streams(s)
-        st[s] = build_ms(eng, D, reps)
-    best_s = min(st, key=st.get)
+    for merged in (False, True):
+        eng.set_merge_sp(merged)
+        for s in streams:
+            eng.set_streams(s)
+            st[(s, merged)] = build_ms(eng, D, reps)
+    best_s, best_m = min(st, key=st.get)
     eng.set_streams(best_s)
-    return {"ms_default": ms_default, "ms_tuned": st[best_s], "streams": st, "best_streams": best_s,
-            "warps": chosen, "class_ms": per}
+    eng.set_merge_sp(best_m)
+    return {"ms_default": ms_default, "ms_tuned": st[(best_s, best_m)],
+            "streams": {s: t for (s, m), t in st.items() if not m},
+            "streams_merged_sp": {s: t for (s, m), t in st.items() if m},
+            "best_streams": best_s, "merge_sp": best_m, "warps": chosen, "class_ms": per}
 
 
 def tune_precision(make_rhf, bounds=(1e-6, 1e-5, 1e-4), tol: float = 1e-6, denserms: float = 1e-7,

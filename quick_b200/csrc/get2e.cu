@@ -579,11 +579,42 @@ constexpr int kMaxLaneWarps = 8;
 // w = 1 for the mixed form's FP32 quartets.
 // FP32 = true: the mixed form's small-bound items (VRR and contraction in FP32),
 // compiled apart so that the FP64 items keep their register budget and vice versa.
+// One work item of a per-lane class (the warp's bra pair against up to 32 kets,
+// one quartet per lane), J of the bra pair summed over the warp.
+template <int La, int Lb, int Lc, int Ld, bool FP32>
+__device__ __forceinline__ void lane_item(const DevData& d, const double2* __restrict__ bt, const int4 w,
+                                          int lane) {
+    using Cls = EriClass<La, Lb, Lc, Ld>;
+    constexpr int NAB = Cls::NA * Cls::NB;
+    double jab[NAB];
+#pragma unroll
+    for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
+    int nq = 0, np = 0;
+    if (lane < w.z) fock_quartet<La, Lb, Lc, Ld, FP32>(d, bt, w.x, w.y + lane, jab, &nq, &np);
+    if (d.stats) {
+        const unsigned sq = __reduce_add_sync(0xffffffffu, (unsigned)nq);
+        const unsigned sp = __reduce_add_sync(0xffffffffu, (unsigned)np);
+        if (lane == 0) {
+            atomicAdd(d.stats, (unsigned long long)sq);
+            atomicAdd(d.stats + 1, (unsigned long long)sp);
+        }
+    }
+    if (d.exchange_only) return;   // no J part
+    const int P = w.x;
+    const int qa = d.pr_qa[P], qb = d.pr_qb[P];
+    const int fa = d.q_f0[qa], fb = d.q_f0[qb];
+#pragma unroll
+    for (int i = 0; i < NAB; ++i) {
+        const double s = warp_sum(jab[i]);
+        if (lane == 0 && s != 0.0)
+            atomic_fixed(d.A + (size_t)(fa + i / Cls::NB) * d.nbasis + fb + i % Cls::NB, s);
+    }
+}
+
 template <int La, int Lb, int Lc, int Ld, bool FP32>
 __global__ void __maxnreg__((EriClass<La, Lb, Lc, Ld>::LANE_REGS))
 fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* __restrict__ counter) {
     using Cls = EriClass<La, Lb, Lc, Ld>;
-    constexpr int NAB = Cls::NA * Cls::NB;
     const int lane = threadIdx.x & 31;
     const double2* bt = class_boys_rows<Cls::M>(d.boys8);
     for (;;) {
@@ -591,32 +622,53 @@ fock_class_kernel(DevData d, const int4* __restrict__ items, int n_items, int* _
         if (lane == 0) it = atomicAdd(counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= n_items) break;
-        const int4 w = items[it];
-        double jab[NAB];
-#pragma unroll
-        for (int i = 0; i < NAB; ++i) jab[i] = 0.0;
-        int nq = 0, np = 0;
-        if (lane < w.z) fock_quartet<La, Lb, Lc, Ld, FP32>(d, bt, w.x, w.y + lane, jab, &nq, &np);
-        if (d.stats) {
-            const unsigned sq = __reduce_add_sync(0xffffffffu, (unsigned)nq);
-            const unsigned sp = __reduce_add_sync(0xffffffffu, (unsigned)np);
-            if (lane == 0) {
-                atomicAdd(d.stats, (unsigned long long)sq);
-                atomicAdd(d.stats + 1, (unsigned long long)sp);
-            }
+        lane_item<La, Lb, Lc, Ld, FP32>(d, bt, items[it], lane);
+    }
+}
+
+// The s/p classes in one persistent kernel (qk_set_merge_sp): the six per-lane s/p
+// classes' item lists joined into one virtual list, heaviest class first, walked
+// with one atomic counter; a warp finds its item's class by binary search over the
+// segments' prefix counts and runs that class's straight-line code.  One launch
+// instead of six, at the register allocation of the largest of the six.
+struct MergedSeg {
+    const int4* items;
+    int begin;   // items of the joined list before this segment
+    int cls;     // position in kSpMerged
+};
+constexpr int kSpMergedN = 6;
+constexpr int kSpMerged[kSpMergedN][4] = {{1, 1, 1, 1}, {1, 1, 1, 0}, {1, 1, 0, 0}, {1, 0, 1, 0}, {1, 0, 0, 0},
+                                          {0, 0, 0, 0}};
+
+#if QK_MAX_L >= 1
+template <bool FP32>
+__global__ void __launch_bounds__(32 * kMaxLaneWarps)
+fock_merged_sp_kernel(DevData d, const MergedSeg* __restrict__ segs, int nseg, int n_items,
+                      int* __restrict__ counter) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= n_items) break;
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].begin <= it) lo = mid; else hi = mid - 1;
         }
-        if (d.exchange_only) continue;   // no J part
-        const int P = w.x;
-        const int qa = d.pr_qa[P], qb = d.pr_qb[P];
-        const int fa = d.q_f0[qa], fb = d.q_f0[qb];
-#pragma unroll
-        for (int i = 0; i < NAB; ++i) {
-            const double s = warp_sum(jab[i]);
-            if (lane == 0 && s != 0.0)
-                atomic_fixed(d.A + (size_t)(fa + i / Cls::NB) * d.nbasis + fb + i % Cls::NB, s);
+        const MergedSeg sg = segs[lo];
+        const int4 w = sg.items[it - sg.begin];
+        switch (sg.cls) {
+            case 0: lane_item<1, 1, 1, 1, FP32>(d, class_boys_rows<EriClass<1, 1, 1, 1>::M>(d.boys8), w, lane); break;
+            case 1: lane_item<1, 1, 1, 0, FP32>(d, class_boys_rows<EriClass<1, 1, 1, 0>::M>(d.boys8), w, lane); break;
+            case 2: lane_item<1, 1, 0, 0, FP32>(d, class_boys_rows<EriClass<1, 1, 0, 0>::M>(d.boys8), w, lane); break;
+            case 3: lane_item<1, 0, 1, 0, FP32>(d, class_boys_rows<EriClass<1, 0, 1, 0>::M>(d.boys8), w, lane); break;
+            case 4: lane_item<1, 0, 0, 0, FP32>(d, class_boys_rows<EriClass<1, 0, 0, 0>::M>(d.boys8), w, lane); break;
+            default: lane_item<0, 0, 0, 0, FP32>(d, class_boys_rows<EriClass<0, 0, 0, 0>::M>(d.boys8), w, lane); break;
         }
     }
 }
+#endif
 
 
 // Batched (many-molecule) variants.  Per class, the work of every molecule stays
@@ -1160,6 +1212,12 @@ struct qk_ctx {
     qk::DevBuf<char> d_wl;             // scratch of the device work-list builder
     bool worklist_on_device = true;    // qk_set_worklist_builder
     int launches = 0;
+    // qk_set_merge_sp: the s/p classes in one launch per precision
+    bool merge_sp = false;
+    bool m_ready = false;              // tables below follow the current lists
+    qk::DevBuf<qk::MergedSeg> d_mseg;  // FP64 segments, then FP32 segments
+    int m_nseg[2] = {}, m_items[2] = {}, m_grid[2] = {}, m_block = 0, m_launches = 0;
+    bool m_class[qk::kNumClasses] = {};   // classes the merged launches cover
     long long last_quart = 0, last_primq = 0;
     int num_sms = 148;
     // device buffers
@@ -1782,6 +1840,65 @@ static int ensure_pairs(qk_ctx* c) {
     c->built_cut = c->integralCutoff;
     c->built_fp32 = c->fp32_bound;
     c->pairs_dirty = false;
+    c->m_ready = false;
+    return QK_OK;
+}
+
+// The segment tables and launch shapes of the merged s/p launches for the current
+// lists (qk_set_merge_sp); m_launches = the build's launches with them.
+static int prepare_merged(qk_ctx* c) {
+#if QK_MAX_L >= 1
+    std::vector<MergedSeg> segs[2];
+    int total[2] = {0, 0};
+    for (int k = 0; k < kNumClasses; ++k) c->m_class[k] = false;
+    int replaced = 0;
+    for (int m = 0; m < kSpMergedN; ++m) {
+        int ci = -1;
+        for (int k = 0; k < kNumClasses; ++k)
+            if (g_classes[k].La == kSpMerged[m][0] && g_classes[k].Lb == kSpMerged[m][1] &&
+                g_classes[k].Lc == kSpMerged[m][2] && g_classes[k].Ld == kSpMerged[m][3] && !g_classes[k].coop)
+                ci = k;
+        if (ci < 0) continue;
+        const ClassWork& W = c->work[ci];
+        c->m_class[ci] = true;
+        replaced += (W.n64 > 0) + (W.n64 < W.n_items);
+        const int n[2] = {W.n64, W.n_items - W.n64};
+        const int4* it[2] = {W.d_items, W.d_items + W.n64};
+        for (int part = 0; part < 2; ++part)
+            if (n[part] > 0) {
+                segs[part].push_back({it[part], total[part], m});
+                total[part] += n[part];
+            }
+    }
+    std::vector<MergedSeg> all(segs[0]);
+    all.insert(all.end(), segs[1].begin(), segs[1].end());
+    if (!all.empty()) {
+        QK_CUDA_TRY(c->d_mseg.upload(all, c->stream));
+        QK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
+    const int wpb = kWarpsPerBlock;
+    c->m_block = 32 * wpb;
+    int parts = 0;
+    for (int part = 0; part < 2; ++part) {
+        c->m_nseg[part] = (int)segs[part].size();
+        c->m_items[part] = total[part];
+        c->m_grid[part] = 0;
+        if (total[part] == 0) continue;
+        int bps = 0;
+        const void* fn = part ? (const void*)fock_merged_sp_kernel<true> : (const void*)fock_merged_sp_kernel<false>;
+        QK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, c->m_block, 0));
+        if (bps < 1) return fail(QK_ERR_CUDA, "merged s/p kernel cannot be resident");
+        c->m_grid[part] = (int)std::max<long long>(1, std::min<long long>((long long)bps * c->num_sms,
+                                                                          (total[part] + wpb - 1) / wpb));
+        ++parts;
+    }
+    c->m_launches = c->launches - replaced + parts;
+#else
+    for (int k = 0; k < kNumClasses; ++k) c->m_class[k] = false;
+    c->m_nseg[0] = c->m_nseg[1] = c->m_items[0] = c->m_items[1] = 0;
+    c->m_launches = c->launches;
+#endif
+    c->m_ready = true;
     return QK_OK;
 }
 
@@ -1816,12 +1933,18 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
         QK_CUDA_TRY(cudaGetLastError());
         cutmat = c->d_cutmat.p;
     }
-    QK_CUDA_TRY(c->d_counters.reserve(2 * kNumClasses));
+    // merged s/p launches: not when every class is timed or counted on its own
+    const bool merged = c->merge_sp && !c->profile_events && !c->profile_stats;
+    if (merged && !c->m_ready) {
+        st = prepare_merged(c);
+        if (st) return st;
+    }
+    QK_CUDA_TRY(c->d_counters.reserve(2 * kNumClasses + 2));
     if (!A_ext) {
         QK_CUDA_TRY(c->d_A.reserve((size_t)n * n));
         QK_CUDA_TRY(cudaMemsetAsync(c->d_A.p, 0, sizeof(unsigned long long) * n * n, s));
     }
-    QK_CUDA_TRY(cudaMemsetAsync(c->d_counters.p, 0, sizeof(int) * 2 * kNumClasses, s));
+    QK_CUDA_TRY(cudaMemsetAsync(c->d_counters.p, 0, sizeof(int) * (2 * kNumClasses + 2), s));
     DevData d = make_devdata(c);
     d.D = D;
     d.cutmat = cutmat;
@@ -1839,11 +1962,33 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     // remaining SMs).  With per-class event timing on they run one after another
     // on `s`, so that every class kernel is timed alone.
     const bool concurrent = !c->profile_events && c->nstreams > 0;
+#if QK_MAX_L >= 1
+    if (merged) {
+        // the joined s/p lists first, on the caller's stream
+        for (int part = 0; part < 2; ++part)
+            if (c->m_items[part] > 0) {
+                const MergedSeg* sg = c->d_mseg.p + (part ? c->m_nseg[0] : 0);
+                int* ctr = c->d_counters.p + 2 * kNumClasses + part;
+                if (part)
+                    fock_merged_sp_kernel<true><<<c->m_grid[1], c->m_block, 0, s>>>(d, sg, c->m_nseg[1],
+                                                                                  c->m_items[1], ctr);
+                else
+                    fock_merged_sp_kernel<false><<<c->m_grid[0], c->m_block, 0, s>>>(d, sg, c->m_nseg[0],
+                                                                                   c->m_items[0], ctr);
+                QK_CUDA_TRY(cudaGetLastError());
+            }
+    }
+#endif
     if (concurrent) QK_CUDA_TRY(cudaEventRecord(c->fork_ev, s));
     bool used[qk_ctx::kAux] = {};
     int slot = 0;
     for (int ci : c->launch_order) {
         ClassWork& W = c->work[ci];
+        if (merged && c->m_class[ci]) {
+            nq += W.nquart;
+            npq += W.nprimq;
+            continue;
+        }
         cudaStream_t ls = s;
         if (concurrent) {
             const int k = slot++ % c->nstreams;
@@ -2697,15 +2842,28 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     return QK_OK;
 }
 
+// kernel launches of one build with the current lists and settings
+static int build_launches(const qk_ctx* c) {
+    return (c->merge_sp && c->m_ready && !c->profile_events && !c->profile_stats) ? c->m_launches : c->launches;
+}
+
 int qk_last_work(qk_ctx* c, long long* quartets, long long* primq, int* launches) {
     if (!c) return fail(QK_ERR_INVALID_ARG, "null context");
     if (quartets) *quartets = c->last_quart;
     if (primq) *primq = c->last_primq;
-    if (launches) *launches = c->launches;
+    if (launches) *launches = build_launches(c);
     return QK_OK;
 }
 
-int qk_launches_per_build(qk_ctx* c) { return c ? c->launches : 0; }
+int qk_launches_per_build(qk_ctx* c) { return c ? build_launches(c) : 0; }
+
+int qk_set_merge_sp(qk_ctx* c, int on) {
+    if (!c || (on != 0 && on != 1)) return fail(QK_ERR_INVALID_ARG, "qk_set_merge_sp: 0 or 1");
+    std::lock_guard<std::mutex> g(c->mu);
+    c->merge_sp = on == 1;
+    c->m_ready = false;
+    return QK_OK;
+}
 
 int qk_set_class_launch(qk_ctx* c, int ci, int warps_per_block, int blocks_per_sm) {
     if (!c || ci < 0 || ci >= kNumClasses) return fail(QK_ERR_INVALID_ARG, "qk_set_class_launch: class index");

@@ -226,6 +226,10 @@ class Get2e:
         """Build the work lists on the GPU (default) or on the host (same lists)."""
         check(lib().qk_set_worklist_builder(self.h, int(bool(on_device))), "qk_set_worklist_builder")
 
+    def set_merge_sp(self, on: bool):
+        """The s/p classes as one persistent kernel per precision (qk_set_merge_sp)."""
+        check(lib().qk_set_merge_sp(self.h, 1 if on else 0), "qk_set_merge_sp")
+
     def set_streams(self, nstreams: int):
         """Class kernels over ``nstreams`` concurrent streams (0: one after another)."""
         check(lib().qk_set_streams(self.h, int(nstreams)), "qk_set_streams")

@@ -123,10 +123,29 @@ def _point_charges(rng, qm_xyz_bohr, n, radius_ang, exclude_ang=2.0):
     return np.array(pos), np.array(q)
 
 
+def _independent_charges(rng, qm_xyz_bohr, n, radius_ang, exclude_ang=2.0):
+    """n independent point charges, each uniform in a sphere of ``radius_ang``
+    around the QM centroid and at least ``exclude_ang`` from every QM atom: a third
+    with the TIP3P oxygen charge (-0.834 e), the rest with the hydrogen charge
+    (+0.417 e), so the set is about neutral but has no local (molecular) neutrality."""
+    c = qm_xyz_bohr.mean(axis=0)
+    R = radius_ang * A_TO_BOHRS
+    ex2 = (exclude_ang * A_TO_BOHRS) ** 2
+    pos = []
+    while len(pos) < n:
+        o = rng.uniform(-R, R, size=3)
+        x = c + o
+        if o @ o <= R * R and ((qm_xyz_bohr - x) ** 2).sum(-1).min() >= ex2:
+            pos.append(x)
+    q = np.full(n, TIP3P_H)
+    q[: n // 3] = TIP3P_O
+    return np.array(pos), q
+
+
 def request_stream(n_requests: int, rate: float, seed: int = 20261203, qmmm_fraction: float = 0.25,
                    max_waters: int = 40, bases=("STO-3G", "6-31G*"), qm_waters: int = 20,
                    n_charges: int = 4000, charge_radius: float = 15.0, sigma: float = 0.01,
-                   n_series: int = 16):
+                   n_series: int = 16, charges: str = "waters"):
     """The serving workload: ``n_requests`` RHF requests with Poisson arrivals at
     ``rate`` per second.
 
@@ -136,13 +155,18 @@ def request_stream(n_requests: int, rate: float, seed: int = 20261203, qmmm_frac
       each a ``qm_waters`` QM region with ``n_charges`` TIP3P point charges (MM
       waters, :func:`_point_charges`) within ``charge_radius`` A; every repeat
       moves the QM atoms and the charges of its series by Gaussian ``sigma`` A (a
-      random walk), and is solved from the series' last density.
+      random walk), and is solved from the series' last density.  ``charges``:
+      "waters" (the default) places the charges as rigid TIP3P waters;
+      "independent" places each charge on its own (:func:`_independent_charges`).
     """
+    if charges not in ("waters", "independent"):
+        raise ValueError("charges: 'waters' or 'independent'")
+    place = _point_charges if charges == "waters" else _independent_charges
     rng = np.random.Generator(np.random.PCG64(seed))
     series = []
     for s in range(n_series):
         mol = water_cluster(qm_waters, cluster_box(qm_waters), seed=seed + 7919 * (s + 1))
-        pos, q = _point_charges(rng, mol.xyz, n_charges, charge_radius)
+        pos, q = place(rng, mol.xyz, n_charges, charge_radius)
         series.append({"mol": mol, "pos": pos, "q": q, "basis": bases[s % len(bases)]})
     out = []
     t = 0.0
@@ -719,11 +743,11 @@ def _max_dE(results, ref_E):
 
 def run_stream(n_requests: int, rate: float, fp32_bound: float = 0.0, seed: int = 20261203,
                memory_budget: int = None, denserms: float = 1e-6, device: int = 0, workers: int = 4, lanes: int = 4,
-               **stream_kw):
+               maxiter: int = 100, **stream_kw):
     """Serve one seeded stream; returns (summary dict, results)."""
     reqs = request_stream(n_requests, rate, seed=seed, **stream_kw)
     srv = Server(device=device, memory_budget=memory_budget, fp32_bound=fp32_bound, denserms=denserms,
-                 workers=workers, lanes=lanes)
+                 workers=workers, lanes=lanes, maxiter=maxiter)
     try:
         res = srv.serve(reqs, realtime=True)
         s = summarize(res, srv.wall)
@@ -757,6 +781,9 @@ def main(argv=None):
     ap.add_argument("--budget-gb", type=float, default=None)
     ap.add_argument("--workers", type=int, default=4, help="set-up threads")
     ap.add_argument("--lanes", type=int, default=4, help="streams the post-build graphs are spread over")
+    ap.add_argument("--charges", default="waters", choices=["waters", "independent"],
+                    help="QM/MM point charges as rigid TIP3P waters or as independent charges")
+    ap.add_argument("--maxiter", type=int, default=100)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--out", default=None)
     ap.add_argument("--warmup", type=int, default=64,
@@ -767,20 +794,22 @@ def main(argv=None):
     a = ap.parse_args(argv)
     budget = int(a.budget_gb * (1 << 30)) if a.budget_gb else None
     if a.warmup > 0:
-        w = Server(memory_budget=budget, workers=a.workers, lanes=a.lanes)
+        w = Server(memory_budget=budget, workers=a.workers, lanes=a.lanes, maxiter=a.maxiter)
         w.serve(request_stream(a.warmup, 1000.0, seed=a.seed + 1), realtime=False)
         w.close()
     report = []
     seq = None
     if a.sequential:
-        seq, rseq = run_sequential(request_stream(a.requests, 1.0, seed=a.seed))
+        seq, rseq = run_sequential(request_stream(a.requests, 1.0, seed=a.seed, charges=a.charges), maxiter=a.maxiter)
         print(json.dumps({"sequential_fp64": seq}), flush=True)
         report.append({"sequential_fp64": seq})
     for rate in a.rate:
         if a.compare:
-            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget, workers=a.workers, lanes=a.lanes)
+            s64, r64 = run_stream(a.requests, rate, 0.0, a.seed, budget, workers=a.workers, lanes=a.lanes,
+                                  maxiter=a.maxiter, charges=a.charges)
             bound = a.fp32_bound if a.fp32_bound > 0 else 1e-5
-            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget, workers=a.workers, lanes=a.lanes)
+            s32, r32 = run_stream(a.requests, rate, bound, a.seed, budget, workers=a.workers, lanes=a.lanes,
+                                  maxiter=a.maxiter, charges=a.charges)
             e64 = {r.rid: r.E for r in r64}
             dE = [abs(r.E - e64[r.rid]) for r in r32 if r.rid in e64]
             s32["max_abs_dE_vs_fp64"] = float(max(dE)) if dE else None
@@ -793,7 +822,8 @@ def main(argv=None):
                 line["mixed_vs_sequential_fp64"] = s32["solves_per_s"] / seq["solves_per_s"]
                 line["fp64_vs_sequential_fp64"] = s64["solves_per_s"] / seq["solves_per_s"]
         else:
-            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget, workers=a.workers, lanes=a.lanes)
+            line, res = run_stream(a.requests, rate, a.fp32_bound, a.seed, budget, workers=a.workers, lanes=a.lanes,
+                                   maxiter=a.maxiter, charges=a.charges)
             if seq:
                 line["vs_sequential_fp64"] = line["solves_per_s"] / seq["solves_per_s"]
         print(json.dumps(line), flush=True)

@@ -47,7 +47,8 @@ def test_tune_applies_the_fastest_shape():
     ref = eng.fock2e(D).cpu().numpy()
     rep = at.tune(eng, D, warps=(2, 4), streams=(0, 4), reps=2)
     assert rep["best_streams"] in (0, 4)
-    assert rep["ms_tuned"] == min(rep["streams"].values())
+    assert rep["ms_tuned"] == min(list(rep["streams"].values()) + list(rep["streams_merged_sp"].values()))
+    assert rep["merge_sp"] in (False, True)
     for name, w in rep["warps"].items():
         assert w == min(rep["class_ms"][name], key=rep["class_ms"][name].get)
     assert eng.fock2e(D).cpu().numpy().tobytes() == ref.tobytes()

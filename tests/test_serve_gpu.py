@@ -170,3 +170,27 @@ def test_realtime_stream_reports_latency():
     assert s["requests"] == 24 and s["converged"] == 24
     assert 0 < s["p50_ms"] <= s["p99_ms"]
     assert all(r.done >= r.arrival for r in res)
+
+
+def test_served_energies_match_oracle_scf():
+    """Each request of a served mix -- plain FP64 and the mixed form (FP32 below a
+    Schwarz bound product of 1e-5) -- against the oracle's RHF of the same molecule
+    (and point charges) at the same cutoffs, converged tightly: the mixed form
+    within 1 uEh per request (the serving target's bound), plain FP64 within 1e-7
+    Eh (the plain path's bound against the reference CPU path)."""
+    _cuda()
+    from oracle import oracle as O
+    reqs = _mix()
+    out = {}
+    for bound in (0.0, 1e-5):
+        srv = Server(fp32_bound=bound)
+        out[bound] = srv.serve(reqs, realtime=False)
+        srv.close()
+    for r in reqs:
+        b = build_basis(r.mol, r.basis)
+        ref = O.rhf(b, integral_cutoff=1e-10, prim_limit=1e-11, conv=1e-9, ext_charges=r.ext_charges)
+        e64, e32 = out[0.0][r.rid].E, out[1e-5][r.rid].E
+        print(f"rid {r.rid} ({r.kind}, {r.basis}, {b.nbasis} bf): |dE| fp64 {abs(e64 - ref['E']):.2e}, "
+              f"mixed {abs(e32 - ref['E']):.2e}")
+        assert abs(e64 - ref["E"]) <= 1e-7, (r.rid, e64, ref["E"])
+        assert abs(e32 - ref["E"]) <= 1e-6, (r.rid, e32, ref["E"])
