@@ -680,7 +680,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg (1 GPU only)")
-    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-requests", type=int, default=1024)
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)

@@ -749,6 +749,26 @@ fock_coop_kernel_batch(const DevData* __restrict__ dl, const BatchSeg* __restric
     }
 }
 
+// The per-lane kernels of the s/p classes, single-molecule and batched, FP64 and FP32.
+// When the build compiles them in their own translation unit (fock_lane_sp.cu,
+// QK_LANE_SP_TU_SEPARATE), this unit only declares them.
+#define QK_LANE_SP_CLASSES(X) X(0, 0, 0, 0) X(1, 0, 0, 0) X(1, 0, 1, 0) X(1, 1, 0, 0) X(1, 1, 1, 0) X(1, 1, 1, 1)
+#if defined(QK_LANE_SP_TU_SEPARATE) && !defined(QK_LANE_SP_TU) && QK_MAX_L >= 1
+#define QK_LANE_SP_EXTERN(a, b, c, e)                                                                     \
+    extern template __global__ void fock_class_kernel<a, b, c, e, false>(DevData, const int4*, int, int*); \
+    extern template __global__ void fock_class_kernel<a, b, c, e, true>(DevData, const int4*, int, int*);  \
+    extern template __global__ void fock_class_kernel_batch<a, b, c, e, false>(const DevData*, const BatchSeg*, \
+                                                                               int, int, int*);             \
+    extern template __global__ void fock_class_kernel_batch<a, b, c, e, true>(const DevData*, const BatchSeg*,  \
+                                                                              int, int, int*);
+QK_LANE_SP_CLASSES(QK_LANE_SP_EXTERN)
+#undef QK_LANE_SP_EXTERN
+#endif
+
+#ifdef QK_LANE_SP_TU
+}  // namespace qk
+#else
+
 // Per-molecule set-up and finish of a batched build, one launch each for all
 // molecules: grid (chunks, molecules), grid-stride inside a molecule.
 struct BatchMol {
@@ -3155,3 +3175,5 @@ void gpu_delete_(int* ierr) {
 }
 
 }  // extern "C"
+
+#endif  // QK_LANE_SP_TU
