@@ -693,12 +693,15 @@ def summarize(results, wall: float) -> dict:
 
 
 def run_sequential(requests, fp32_bound: float = 0.0, device: int = 0, denserms: float = 1e-6,
-                   integral_cutoff: float = 1e-10, maxiter: int = 100):
+                   integral_cutoff: float = 1e-10, maxiter: int = 100, graph: bool = False):
     """The plain path the server is measured against: the same requests solved one
     at a time, in request order, with no batching -- per request its basis, its
     context (one context rebound to each molecule, as a caller of the one-molecule
     API would keep it), one-electron integrals with its point charges, the SAD
-    guess (or its series' last density) and a graph-captured SCF (``GraphSCF``).
+    guess (or its series' last density) and the device SCF cycle (``GraphSCF``),
+    run eagerly (the default: one request at a time it is the faster form, the
+    capture of two graphs per request costing more than their replays save) or
+    captured as CUDA graphs (``graph=True``).
     Returns (summary, results); ``solves_per_s`` is the requests over the time
     to solve all of them back to back, arrivals ignored (the capacity of the
     plain path)."""
@@ -721,7 +724,7 @@ def run_sequential(requests, fp32_bound: float = 0.0, device: int = 0, denserms:
             eng.bind(basis)
         rhf = RHF(basis, device=device, ext_charges=req.ext_charges, engine=eng)
         D0 = series_D.get(req.series) if req.series is not None else None
-        r = GraphSCF(rhf).run(denserms=denserms, maxiter=maxiter, D0=D0)
+        r = GraphSCF(rhf).run(denserms=denserms, maxiter=maxiter, D0=D0, graph=graph)
         if req.series is not None and r["converged"]:
             series_D[req.series] = r["D"]
         done = time.perf_counter() - t0
