@@ -241,7 +241,8 @@ int qk_batch_fock2e(qk_batch *batch, int n, qk_ctx *const *ctx, const double *co
 int qk_batch_reserve_sms(qk_batch *batch, int sms);
 
 /* Work statistics of the last build: shell quartets listed and primitive quartets
- * listed after Schwarz screening (before density screening). */
+ * listed after Schwarz screening (before density screening), and the kernel
+ * launches that build made (before any build: those the next build will make). */
 int qk_last_work(qk_ctx *ctx, long long *quartets, long long *prim_quartets, int *launches);
 /* Kernel launches of one build (for launch accounting). */
 int qk_launches_per_build(qk_ctx *ctx);

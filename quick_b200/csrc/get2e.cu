@@ -1239,6 +1239,7 @@ struct qk_ctx {
     int m_nseg[2] = {}, m_items[2] = {}, m_grid[2] = {}, m_block = 0, m_launches = 0;
     bool m_class[qk::kNumClasses] = {};   // classes the merged launches cover
     long long last_quart = 0, last_primq = 0;
+    int last_launches = 0;             // kernel launches of the last build
     int num_sms = 148;
     // device buffers
     qk::DevBuf<double> d_xyz, d_boys, d_boys8, d_D, d_cutmat, d_o;
@@ -2042,6 +2043,7 @@ static int fock2e_device(qk_ctx* c, const double* D, const double* cutmat, doubl
     }
     c->last_quart = nq;
     c->last_primq = npq;
+    c->last_launches = merged ? c->m_launches : c->launches;
     return QK_OK;
 }
 
@@ -2201,6 +2203,7 @@ static int fock2e_device_noalloc(qk_ctx* c, const double* D, const double* cutma
     QK_CUDA_TRY(cudaGetLastError());
     c->last_quart = nq;
     c->last_primq = npq;
+    c->last_launches = c->launches;   // one launch per class (never the merged s/p kernel)
     return QK_OK;
 }
 
@@ -2871,7 +2874,7 @@ int qk_last_work(qk_ctx* c, long long* quartets, long long* primq, int* launches
     if (!c) return fail(QK_ERR_INVALID_ARG, "null context");
     if (quartets) *quartets = c->last_quart;
     if (primq) *primq = c->last_primq;
-    if (launches) *launches = build_launches(c);
+    if (launches) *launches = c->last_launches ? c->last_launches : build_launches(c);
     return QK_OK;
 }
 

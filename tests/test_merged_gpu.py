@@ -33,3 +33,30 @@ def test_merged_sp_launch_equals_per_class_launches(bas, nw, bound):
     (G0, l0), (G1, l1) = out[False], out[True]
     assert G0[0].tobytes() == G0[1].tobytes() == G1[0].tobytes() == G1[1].tobytes()
     assert l1 < l0, (l0, l1)
+
+
+def test_allocation_free_build_reports_its_own_launches():
+    """With the merged option set, the allocation-free build still launches one
+    kernel per class; qk_last_work reports the launches of the build that ran."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import ctypes
+    from quick_b200._native import check, lib
+    from quick_b200.get2e import Get2e
+    b = build_basis(water_cluster(3, 6.0, seed=6), "STO-3G")
+    rng = np.random.default_rng(12)
+    X = rng.normal(size=(b.nbasis, b.nbasis)) * 0.15
+    D = torch.tensor(X @ X.T / b.nbasis ** 0.5, device="cuda")
+    eng = Get2e(b, integral_cutoff=1e-10, prim_limit=1e-11)
+    eng.set_merge_sp(True)
+    G_merged = eng.fock2e(D).cpu().numpy()
+    merged = eng.work()["launches"]
+    o = torch.zeros_like(D)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib().qk_fock2e_device_noalloc(ctypes.c_void_p(eng.h), ctypes.c_void_p(D.data_ptr()), None,
+                                         ctypes.c_void_p(o.data_ptr()), s), "qk_fock2e_device_noalloc")
+    torch.cuda.synchronize()
+    per_class = eng.work()["launches"]
+    eng.close()
+    assert per_class > merged
+    assert np.abs(o.cpu().numpy() - G_merged).max() == 0.0
