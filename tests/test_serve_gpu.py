@@ -194,3 +194,38 @@ def test_served_energies_match_oracle_scf():
               f"mixed {abs(e32 - ref['E']):.2e}")
         assert abs(e64 - ref["E"]) <= 1e-7, (r.rid, e64, ref["E"])
         assert abs(e32 - ref["E"]) <= 1e-6, (r.rid, e32, ref["E"])
+
+
+def test_pipelined_loop_equals_serial_loop():
+    """Two cohorts stepped in turn (the default) and one batch per step give the
+    same energies, cycle counts and densities, bit for bit."""
+    _cuda()
+    reqs = _mix()
+    out = {}
+    for pipeline in (False, True):
+        srv = Server(keep_densities=True, workers=0, pipeline=pipeline)
+        out[pipeline] = srv.serve(reqs, realtime=False)
+        srv.close()
+    for a, b in zip(out[False], out[True]):
+        assert a.E == b.E and a.niter == b.niter and torch.equal(a.D, b.D), a.rid
+
+
+def test_own_streams_are_reused_not_destroyed():
+    """Streams given back with free_stream are handed out again (torch keeps
+    per-stream allocator state for as long as the process runs)."""
+    _cuda()
+    from quick_b200._native import free_stream, own_stream
+    s1 = own_stream(0)
+    p1 = s1.cuda_stream
+    free_stream(s1)
+    s2 = own_stream(0)
+    assert s2.cuda_stream == p1
+    s3 = own_stream(0)
+    assert s3.cuda_stream != p1
+    x = torch.ones(1000, device="cuda")
+    with torch.cuda.stream(s3):
+        y = x * 2.0
+    torch.cuda.current_stream().wait_stream(s3)
+    assert float(y.sum()) == 2000.0
+    free_stream(s2)
+    free_stream(s3)
