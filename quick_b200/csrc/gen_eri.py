@@ -276,9 +276,11 @@ def class_list(lmax=LMAX):
 # and 103 in another, dpss 128 and 170) and the higher counts cost occupancy; the
 # ceilings below are the fastest of a sweep (no ceiling, 128, 85, 64 and the
 # allocations ptxas chose) measured on 32 H2O / 6-31G*, per class kernel timed
-# alone.  Classes not listed keep ptxas's choice (255 = no ceiling).
+# alone; for the per-lane f classes a 168 ceiling measured on 12 H2O / cc-pVTZ
+# helped fpss (-19%) and slowed the others by 35-50%.  Classes not listed keep
+# ptxas's choice (255 = no ceiling).
 LANE_REGS = {(0, 0, 0, 0): 64, (1, 0, 0, 0): 80, (2, 0, 0, 0): 96, (2, 1, 0, 0): 128, (2, 2, 0, 0): 128,
-             (1, 1, 1, 0): 128, (2, 0, 1, 0): 128}
+             (1, 1, 1, 0): 128, (2, 0, 1, 0): 128, (3, 1, 0, 0): 168}
 
 
 def emit_class(La, Lb, Lc, Ld):
