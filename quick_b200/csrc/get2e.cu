@@ -60,6 +60,14 @@ struct DevData {
     const int* __restrict__ pr_npp;
     const int* __restrict__ pr_pps;      // stride between a pair's primitive pairs
     const double* __restrict__ pr_Y;
+    // per pair, what the per-lane quartet code would otherwise reach through chains
+    // of dependent loads (pair -> Qshell -> parent shell / atom -> coordinates):
+    // (parent shell of a, of b, first function of a, of b); the top angular
+    // momenta of the two shells summed; and (Ax, Ay), (Az, ABx), (ABy, ABz) with A
+    // the centre of the first Qshell and AB = A - B
+    const int4* __restrict__ pr_sh;
+    const int* __restrict__ pr_lt;
+    const double2* __restrict__ pr_geo;   // 3 per pair
     // per primitive pair, five 16-byte fields (one vector load each):
     // (zeta, 1/(2 zeta)), (K, cutprim), (Px, Py), (Pz, PAx), (PAy, PAz) with
     // K = exp(-ab/zeta R_AB^2)/zeta c_a c_b sqrt(X0) and PA = P - centre of the first shell
@@ -168,8 +176,8 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
     constexpr int NA = Cls::NA, NB = Cls::NB, NC = Cls::NC, ND = Cls::ND;
     constexpr int NE = Cls::NE, NF = Cls::NF, NAB = NA * NB;
     const int n = d.nbasis, ns = d.nshell;
-    const int qa = d.pr_qa[P], qb = d.pr_qb[P], qc = d.pr_qa[Q], qd = d.pr_qb[Q];
-    const int sa = d.q_parent[qa], sb = d.q_parent[qb], sc = d.q_parent[qc], sd = d.q_parent[qd];
+    const int4 shP = d.pr_sh[P], shQ = d.pr_sh[Q];
+    const int sa = shP.x, sb = shP.y, sc = shQ.x, sd = shQ.y;
     const double* cm = d.cutmat;
     double dnmax = fmax(4.0 * cm[sa * ns + sb], 4.0 * cm[sc * ns + sd]);
     dnmax = fmax(dnmax, fmax(cm[sa * ns + sd], cm[sa * ns + sc]));
@@ -180,13 +188,13 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
     if (!(ct > d.cut) || !(ct * dnmax > d.cut)) return;
     ++*nq_done;
 
-    const int ia = d.q_atom[qa], ib = d.q_atom[qb], ic = d.q_atom[qc], id = d.q_atom[qd];
-    const double AB[3] = {d.xyz[3 * ia] - d.xyz[3 * ib], d.xyz[3 * ia + 1] - d.xyz[3 * ib + 1],
-                          d.xyz[3 * ia + 2] - d.xyz[3 * ib + 2]};
-    const double Cc[3] = {d.xyz[3 * ic], d.xyz[3 * ic + 1], d.xyz[3 * ic + 2]};
-    const double CD[3] = {Cc[0] - d.xyz[3 * id], Cc[1] - d.xyz[3 * id + 1], Cc[2] - d.xyz[3 * id + 2]};
+    const double2 gp1 = d.pr_geo[3 * P + 1], gp2 = d.pr_geo[3 * P + 2];
+    const double2 gq0 = d.pr_geo[3 * Q], gq1 = d.pr_geo[3 * Q + 1], gq2 = d.pr_geo[3 * Q + 2];
+    const double AB[3] = {gp1.y, gp2.x, gp2.y};
+    const double Cc[3] = {gq0.x, gq0.y, gq1.x};
+    const double CD[3] = {gq1.y, gq2.x, gq2.y};
 
-    const int mq = d.q_ltop[qa] + d.q_ltop[qb] + d.q_ltop[qc] + d.q_ltop[qd];
+    const int mq = d.pr_lt[P] + d.pr_lt[Q];
     double acc[NE * NF];
     if constexpr (FP32) {
         // mixed form: small-bound quartet, vertical recursion and contraction in FP32
@@ -205,9 +213,10 @@ __device__ __forceinline__ void fock_quartet(const DevData& d, const double2* __
 #pragma unroll
     for (int f = 0; f < NF; ++f) Cls::hrr_bra(acc + f * NE, t1 + f * NAB, AB[0], AB[1], AB[2]);
 
-    const int fa = d.q_f0[qa], fb = d.q_f0[qb], fc = d.q_f0[qc], fd = d.q_f0[qd];
-    // degeneracy of the unique quartet (pairs are unordered, bra/ket unordered)
-    const double deg = (qa != qb ? 2.0 : 1.0) * (qc != qd ? 2.0 : 1.0) * (P != Q ? 2.0 : 1.0);
+    const int fa = shP.z, fb = shP.w, fc = shQ.z, fd = shQ.w;
+    // degeneracy of the unique quartet (pairs are unordered, bra/ket unordered);
+    // a pair of two different Qshells starts at two different functions
+    const double deg = (fa != fb ? 2.0 : 1.0) * (fc != fd ? 2.0 : 1.0) * (P != Q ? 2.0 : 1.0);
     const double wJ = d.exchange_only ? 0.0 : 0.25 * deg;   // 2 * deg/8
     const double wK = -0.0625 * deg;                        // -1/2 * deg/8
 
@@ -1108,9 +1117,10 @@ struct PairTable {
     std::vector<double> Y;
     std::vector<double2> zo, kc, pxy, pzax, payz;   // the five 16-byte fields of DevData
     std::vector<Bucket> buckets;
-    DevBuf<int> d_qa, d_qb, d_pp0, d_npp, d_pps;
+    DevBuf<int> d_qa, d_qb, d_pp0, d_npp, d_pps, d_lt;
     DevBuf<double> d_Y;
-    DevBuf<double2> d_zo, d_kc, d_pxy, d_pzax, d_payz;
+    DevBuf<double2> d_zo, d_kc, d_pxy, d_pzax, d_payz, d_geo;
+    DevBuf<int4> d_sh;
     void clear() {
         qa.clear(); qb.clear(); pp0.clear(); npp.clear(); pps.clear(); Y.clear();
         zo.clear(); kc.clear(); pxy.clear(); pzax.clear(); payz.clear(); buckets.clear();
@@ -1213,6 +1223,7 @@ struct qk_ctx {
     int natom = 0, nbasis = 0, nshell = 0, jbasis = 0;
     std::vector<double> xyz;
     std::vector<qk::Qsh> qsh;
+    std::vector<int> q_ltop_h;          // per Qshell: the top angular momentum of its shell (1 for SP)
     std::vector<int> shell_f0, shell_f1, shell_prim0;
     bool have_basis = false, have_schwarz = false;
     std::vector<double> Ycut, cutprim;   // nshell^2, jbasis^2 (symmetric)
@@ -1331,6 +1342,9 @@ static DevData make_devdata(qk_ctx* c) {
     d.pr_npp = c->pairs.d_npp.p;
     d.pr_pps = c->pairs.d_pps.p;
     d.pr_Y = c->pairs.d_Y.p;
+    d.pr_sh = c->pairs.d_sh.p;
+    d.pr_lt = c->pairs.d_lt.p;
+    d.pr_geo = c->pairs.d_geo.p;
     d.pp_zo = c->pairs.d_zo.p;
     d.pp_kc = c->pairs.d_kc.p;
     d.pp_pxy = c->pairs.d_pxy.p;
@@ -1453,6 +1467,27 @@ static int upload_pairs(qk_ctx* c) {
     QK_CUDA_TRY(T.d_pxy.upload(T.pxy, s));
     QK_CUDA_TRY(T.d_pzax.upload(T.pzax, s));
     QK_CUDA_TRY(T.d_payz.upload(T.payz, s));
+    // per-pair records of DevData (pr_sh, pr_lt, pr_geo)
+    const size_t np = T.qa.size();
+    std::vector<int4> sh(np);
+    std::vector<int> lt(np);
+    std::vector<double2> geo(3 * np);
+    for (size_t p = 0; p < np; ++p) {
+        const Qsh& a = c->qsh[T.qa[p]];
+        const Qsh& b = c->qsh[T.qb[p]];
+        sh[p] = make_int4(a.parent, b.parent, a.f0, b.f0);
+        lt[p] = c->q_ltop_h[T.qa[p]] + c->q_ltop_h[T.qb[p]];
+        const double* A = &c->xyz[3 * a.atom];
+        const double* B = &c->xyz[3 * b.atom];
+        geo[3 * p] = make_double2(A[0], A[1]);
+        geo[3 * p + 1] = make_double2(A[2], A[0] - B[0]);
+        geo[3 * p + 2] = make_double2(A[1] - B[1], A[2] - B[2]);
+    }
+    QK_CUDA_TRY(T.d_sh.upload(sh, s));
+    QK_CUDA_TRY(T.d_lt.upload(lt, s));
+    QK_CUDA_TRY(T.d_geo.upload(geo, s));
+    // the host vectors die here: the uploads must be done before they go
+    QK_CUDA_TRY(cudaStreamSynchronize(s));
     return QK_OK;
 }
 
@@ -2397,6 +2432,7 @@ int qk_set_basis(qk_ctx* c, int natom, const double* xyz, int nshell, int nbasis
     QK_CUDA_TRY(c->d_q_f0.upload(q_f0, s));
     QK_CUDA_TRY(c->d_q_parent.upload(q_parent, s));
     QK_CUDA_TRY(c->d_q_ltop.upload(q_ltop, s));
+    c->q_ltop_h = q_ltop;
     QK_CUDA_TRY(c->d_q_prim0.upload(q_prim0, s));
     QK_CUDA_TRY(c->d_q_nprim.upload(q_nprim, s));
     QK_CUDA_TRY(c->d_shell_f0.upload(c->shell_f0, s));
@@ -2855,7 +2891,7 @@ int qk_device_bytes(qk_ctx* c, unsigned long long* total, unsigned long long* it
     unsigned long long t = it;
     for (size_t b : {T.d_qa.bytes(), T.d_qb.bytes(), T.d_pp0.bytes(), T.d_npp.bytes(), T.d_pps.bytes(),
                      T.d_Y.bytes(), T.d_zo.bytes(), T.d_kc.bytes(), T.d_pxy.bytes(), T.d_pzax.bytes(),
-                     T.d_payz.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
+                     T.d_payz.bytes(), T.d_sh.bytes(), T.d_lt.bytes(), T.d_geo.bytes(), c->d_xyz.bytes(), c->d_boys.bytes(), c->d_boys8.bytes(), c->d_schwarz_Y.bytes(), c->d_schwarz_cp.bytes(), c->d_D.bytes(), c->d_cutmat.bytes(),
                      c->d_o.bytes(), c->d_q_atom.bytes(), c->d_q_f0.bytes(), c->d_q_parent.bytes(), c->d_q_ltop.bytes(),
                      c->d_q_prim0.bytes(), c->d_q_nprim.bytes(), c->d_shell_f0.bytes(), c->d_shell_f1.bytes(),
                      c->d_A.bytes(), c->d_A2.bytes(), c->d_uhf.bytes(), c->d_counters.bytes(), c->d_stats.bytes()})
